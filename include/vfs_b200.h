@@ -1,0 +1,171 @@
+/*
+ * vfs_b200.h — C ABI of the B200 variational fisheye stereo library
+ * (libvfs_b200.so).
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (cudaStream_t passed as void*), enqueues its work on that stream without
+ * synchronising, allocates no device memory, and returns an int status
+ * (VFS_OK or one of VFS_ERR_*).  vfs_last_error() returns a message for the
+ * last failure on the calling thread.
+ *
+ * Layouts follow the reference (eshibusawa/VFS-Python): C-contiguous arrays,
+ * float2 (H, W, 2), float3 (H, W, 3) array-of-structures, u8 masks (nonzero =
+ * valid).  Each entry point names the reference interface it replaces.
+ */
+#ifndef VFS_B200_H_
+#define VFS_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define VFS_API __attribute__((visibility("default")))
+#else
+#define VFS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VFS_OK 0
+#define VFS_ERR_ARG 1       /* bad pointer, size, shape or parameter */
+#define VFS_ERR_ALIGN 2     /* pointer or pitch misaligned for a texture */
+#define VFS_ERR_WORKSPACE 3 /* workspace missing or too small */
+#define VFS_ERR_CUDA 4      /* a CUDA call failed; see vfs_last_error() */
+#define VFS_ERR_STATE 5     /* call order violated (e.g. solve before set_mask) */
+
+/* Solver parameters: the attributes of the reference's vfs_params
+ * (Python/vfs_params.py:25-43).  All values are run-time arguments; the
+ * reference bakes most of them into its CUDA source (Python/vfs.py:57-68). */
+typedef struct VfsParams {
+  int width, height;
+  double beta, gamma, alpha0, alpha1, timeStepLambda, Lambda, fScale, limitRange;
+  int nLevel, nWarpIters, nSolverIters;
+} VfsParams;
+
+/* Texture kinds for vfs_texture_create. */
+#define VFS_TEX_U8 0
+#define VFS_TEX_F32 2
+#define VFS_TEX_F32X2 3
+
+VFS_API const char* vfs_last_error(void);
+VFS_API int vfs_version(void);
+
+/* ---- texture objects ------------------------------------------------------
+ * Replaces create_texture_object (Python/texture.py:27-55).  The texture is
+ * bound to the caller's pitch-linear buffer (no copy); `ptr` must be
+ * 512-byte aligned and `pitch_bytes` a multiple of 32.  Addressing is mirror
+ * with normalised coordinates, linear filtering when `linear` is nonzero
+ * (point otherwise), as Python/vfs.py:96-98 and :169-171 set up. */
+VFS_API int vfs_texture_create(const void* ptr, int height, int width, size_t pitch_bytes, int kind, int linear,
+                       uint64_t* tex_out);
+VFS_API int vfs_texture_destroy(uint64_t tex);
+
+/* ---- one entry per reference kernel (Python/vfs.cu) -------------------------
+ * Outputs and non-texture inputs are C-contiguous; `mask` is a u8 plane with
+ * row pitch `mask_pitch` bytes.  Names follow the VFS methods that launch
+ * the kernels (Python/vfs.py:93-559). */
+/* castAndScale, Python/vfs.py:127-144 */
+VFS_API int vfs_cast_and_scale(float* out, const uint8_t* in, int h, int w, void* stream);
+/* downSamplingImage / downSamplingVectorField / downSamplingMask,
+ * Python/vfs.py:100-115, 164-181, 195-211; h, w are the coarse size */
+VFS_API int vfs_downsample_image(float* out, uint64_t src_tex, int h, int w, void* stream);
+VFS_API int vfs_downsample_vector_field(float* out_hw2, uint64_t src_tex, int h, int w, void* stream);
+VFS_API int vfs_downsample_mask(uint8_t* out, uint64_t src_tex, int h, int w, void* stream);
+/* warpingImage, Python/vfs.py:220-236 */
+VFS_API int vfs_warping_image(float* out, const float* warp_hw2, uint64_t src_tex, int h, int w, void* stream);
+/* gaussianMasked, Python/vfs.py:238-253 */
+VFS_API int vfs_gaussian(float* out, uint64_t src_tex, const uint8_t* mask, size_t mask_pitch, int h, int w, void* stream);
+/* computeTensorEtaMasked, Python/vfs.py:255-275 */
+VFS_API int vfs_compute_tensor_eta(float* abc_hw3, float* eta_hw3, uint64_t src_tex, const uint8_t* mask, size_t mask_pitch,
+                           const VfsParams* prm, int h, int w, void* stream);
+/* findWarpingVector, Python/vfs.py:277-293 */
+VFS_API int vfs_find_warping_vector(float* out_hw2, const float* warp_hw2, uint64_t field_tex, int h, int w, void* stream);
+/* computeDerivatives, Python/vfs.py:295-313 */
+VFS_API int vfs_compute_derivatives(float* out_hw2, uint64_t ref_tex, uint64_t other_tex, uint64_t field_tex, int h, int w,
+                            void* stream);
+/* updateDualVariables, Python/vfs.py:315-335 (p, q updated in place) */
+VFS_API int vfs_update_dual_variables(float* p_hw2, float* tp_hw2, float* q_hw4, float sigma, const float* u,
+                              const float* v_hw2, const float* abc_hw3, const uint8_t* mask, size_t mask_pitch,
+                              const VfsParams* prm, int h, int w, void* stream);
+/* l1Thresholding, Python/vfs.py:337-357 */
+VFS_API int vfs_l1_thresholding(float* out, float tau, const float* tp_hw2, const float* u, const float* u_,
+                        const float* deriv_hw2, const float* eta_hw3, const uint8_t* mask, size_t mask_pitch,
+                        const VfsParams* prm, int h, int w, void* stream);
+/* updatePrimalVariables, Python/vfs.py:359-382 */
+VFS_API int vfs_update_primal_variables(float* u_out, float* v_out_hw2, float tau, float mu, const float* p_hw2,
+                                const float* q_hw4, const float* u, const float* u_, const float* v_hw2,
+                                const float* abc_hw3, const float* eta_hw3, const uint8_t* mask, size_t mask_pitch,
+                                const VfsParams* prm, int h, int w, void* stream);
+/* medianFilter, Python/vfs.py:384-400 */
+VFS_API int vfs_median_filter(float* out, const float* in, const uint8_t* mask, size_t mask_pitch, int h, int w,
+                      void* stream);
+/* computeOpticalFlowWithClamp, Python/vfs.py:402-418 (warp, u_before in place) */
+VFS_API int vfs_compute_optical_flow_with_clamp(float* warp_hw2, float* u_before, const float* u_filtered,
+                                        const float* tvec_hw2, const uint8_t* mask, size_t mask_pitch,
+                                        const VfsParams* prm, int h, int w, void* stream);
+/* upSamplingVectorField1 / upSamplingVectorField, Python/vfs.py:420-458;
+ * h, w are the fine size */
+VFS_API int vfs_upsampling_vector_field1(float* out, uint64_t src_tex, const VfsParams* prm, int h, int w, void* stream);
+VFS_API int vfs_upsampling_vector_field(float* out_hw2, uint64_t src_tex, const VfsParams* prm, int h, int w, void* stream);
+/* triangulateRays, Python/vfs.py:535-559 (t: 3 floats, host memory) */
+VFS_API int vfs_triangulate_rays(float* out_hw3, const float* rays_hw3, const float* rays_other_hw3, const float* t,
+                         const uint8_t* mask, size_t mask_pitch, int h, int w, void* stream);
+
+/* ---- equidistant camera (Python/equidistant_cam.py, Python/template_cam.cu) */
+/* getRays, Python/equidistant_cam.py:72-92 */
+VFS_API int vfs_cam_get_rays(float* out_hw3, float f, float u0, float v0, int h, int w, void* stream);
+/* getUVFromXYZ, Python/equidistant_cam.py:94-114 */
+VFS_API int vfs_cam_get_uvs(float* out_hw2, const float* xyz_hw3, float f, float u0, float v0, int h, int w, void* stream);
+/* getXYZFromUV, Python/equidistant_cam.py:116-136 */
+VFS_API int vfs_cam_get_xyzs(float* out_hw3, const float* uv_hw2, float f, float u0, float v0, int h, int w, void* stream);
+/* getThetas, Python/equidistant_cam.py:138-159 */
+VFS_API int vfs_cam_get_thetas(float* out_hw3, const float* rays_hw3, int h, int w, void* stream);
+/* getXYZFromDistance, Python/equidistant_cam.py:180-206 */
+VFS_API int vfs_cam_xyz_from_distance(float* out_hw3, const float* rays_hw3, const float* dist, const uint8_t* mask,
+                              size_t mask_pitch, int h, int w, void* stream);
+/* get_vector_fields, Python/vector_field.py:28-56, for the grid of integer
+ * pixel coordinates + grid_offset (0: get_grid_zero, 1: get_grid_one).
+ * R: 9 floats row-major, t: 3 floats, t_scale: 2 floats (host memory). */
+VFS_API int vfs_vector_fields(float* tvf_hw2, float* cvf_hw2, float f_ref, float u0_ref, float v0_ref, float f_other,
+                      float u0_other, float v0_other, const double* R, const double* t, const double* t_scale,
+                      float grid_offset, int h, int w, void* stream);
+
+/* ---- whole solve (Python/vfs.py:84-559) ----------------------------------
+ * A plan owns no memory: the caller provides a workspace of
+ * vfs_plan_workspace_size() bytes (256-byte aligned) that lives as long as
+ * the plan.  Call order mirrors the reference driver
+ * (Python/main_equidistant.py:71-78): set_mask (create_mask_pyramid), then
+ * set_vector_fields (create_vector_field_pyramid), then solve (solve_stereo),
+ * then triangulate (triangulate_flow). */
+typedef struct VfsPlan VfsPlan;
+
+VFS_API int vfs_plan_workspace_size(const VfsParams* prm, size_t* bytes);
+VFS_API int vfs_plan_create(const VfsParams* prm, void* workspace, size_t workspace_bytes, VfsPlan** plan_out);
+VFS_API int vfs_plan_destroy(VfsPlan* plan);
+/* pyramid sizes (compute_pyramid_sizes, Python/vfs.py:84-91): hw_out gets
+ * 2*nLevel ints (h0, w0, h1, w1, ...) */
+VFS_API int vfs_plan_sizes(const VfsPlan* plan, int* hw_out);
+/* create_mask_pyramid, Python/vfs.py:159-187 */
+VFS_API int vfs_plan_set_mask(VfsPlan* plan, const uint8_t* mask, size_t mask_pitch, void* stream);
+/* create_vector_field_pyramid, Python/vfs.py:189-218 */
+VFS_API int vfs_plan_set_vector_fields(VfsPlan* plan, const float* tvf_hw2, const float* cvf_hw2, void* stream);
+/* solve_stereo, Python/vfs.py:460-533; images u8 C-contiguous (H, W);
+ * warp_out (H, W, 2) receives the masked flow */
+VFS_API int vfs_plan_solve(VfsPlan* plan, const uint8_t* img_ref, const uint8_t* img_other, float* warp_out_hw2,
+                   void* stream);
+/* triangulate_flow, Python/vfs.py:535-559, for the flow of the last solve */
+VFS_API int vfs_plan_triangulate(VfsPlan* plan, float f, float u0, float v0, const float* t, float* xyz_out_hw3,
+                         void* stream);
+/* The per-iteration step sizes (sigma, tau, mu) the solve uses, as the
+ * reference's host loop computes them (Python/vfs.py:494-515, NumPy >= 2
+ * scalar rules); out3 receives 3*n floats.  Host-only, no GPU needed. */
+VFS_API int vfs_step_schedule(int n, double time_step_lambda, float* out3);
+/* Select the fused TGV variant (iterations per launch: 1, 2 or 4). */
+VFS_API int vfs_plan_set_tgv_variant(VfsPlan* plan, int iters_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VFS_B200_H_ */

@@ -1,0 +1,383 @@
+// Whole-solve path: a plan that carves a caller-provided workspace into the
+// pyramids, per-warp constants and ping-pong solver state, binds texture
+// objects to the sampled planes once, and enqueues a complete solve_stereo
+// (Python/vfs.py:460-533) on one stream with no host synchronisation.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "vfs_api_util.cuh"
+#include "vfs_kernels.cuh"
+#include "vfs_sample.cuh"
+#include "vfs_tgv.cuh"
+
+namespace vfs {
+namespace {
+
+constexpr size_t kAlign = 512;      // texture base alignment on B200
+constexpr size_t kPitchAlign = 128; // row pitch (texture pitch alignment is 32)
+
+inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+inline size_t pitch_of(int w, size_t esz) { return round_up((size_t)w * esz, kPitchAlign); }
+
+// Bump allocator over the workspace (or a size counter when base is null).
+struct Carver {
+  char* base;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t bytes) {
+    off = round_up(off, kAlign);
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += bytes;
+    return p;
+  }
+};
+
+constexpr int kBX = 32, kBY = 8;
+inline dim3 grid2d(int h, int w) { return dim3((w + kBX - 1) / kBX, (h + kBY - 1) / kBY); }
+
+// computeTensorEtaMasked (Python/vfs.cu:239-281) writing the per-warp
+// constant planes of the fused solver (structure of arrays) and the mask
+// code of each pixel.
+__global__ void k_tensor_soa(TgvConsts out, uint8_t* code, cudaTextureObject_t src, Plane<const uint8_t> mask,
+                             SolverConsts k, int h, int w) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  const int Y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (X >= w || Y >= h) return;
+  const long i = (long)Y * w + X;
+  const uint8_t c = mask_code(mask, X, Y, h, w);
+  code[i] = c;
+  float3 a = make_float3(0, 0, 0), e = make_float3(0, 0, 0);
+  if (c & kSelf) tensor_from_grad(forward_grad(src, X, Y, h, w), k, &a, &e);
+  const_cast<float*>(out.a)[i] = a.x;
+  const_cast<float*>(out.b)[i] = a.y;
+  const_cast<float*>(out.c)[i] = a.z;
+  const_cast<float*>(out.ex)[i] = e.x;
+  const_cast<float*>(out.ey)[i] = e.y;
+  const_cast<float*>(out.ez)[i] = e.z;
+}
+
+// computeDerivatives (Python/vfs.cu:304-324) plus the per-warp solver reset
+// of Python/vfs.py:489-497: p, q, v_ <- 0, u <- u_before, u_ carried over.
+__global__ void k_derivs_init(TgvConsts out, TgvState st, Plane<const float> ubefore, Plane<const float> ub_src,
+                              cudaTextureObject_t tref, cudaTextureObject_t tother, cudaTextureObject_t tdir, int h,
+                              int w) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  const int Y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (X >= w || Y >= h) return;
+  const long i = (long)Y * w + X;
+  const float2 d = epipolar_derivs(tref, tother, tdir, X, Y, h, w);
+  const_cast<float*>(out.iu)[i] = d.x;
+  const_cast<float*>(out.iz)[i] = d.y;
+  const float ubv = ub_src.at(X, Y);
+  st.u[i] = ubefore.at(X, Y);
+  st.ub[i] = ubv;
+  st.vbx[i] = st.vby[i] = 0.f;
+  st.px[i] = st.py[i] = 0.f;
+  st.qx[i] = st.qy[i] = st.qz[i] = st.qw[i] = 0.f;
+}
+
+}  // namespace
+}  // namespace vfs
+
+using namespace vfs;
+
+struct VfsPlan {
+  VfsParams prm;
+  SolverConsts kc;
+  int L = 0;
+  struct Level {
+    int h, w;
+    Plane<float> ref, other;
+    Plane<float2> tvf;
+    Plane<uint8_t> mask;
+    uint8_t* code;
+    cudaTextureObject_t ref_tex = 0, other_tex = 0, tvf_tex = 0, mask_tex = 0, smooth_tex = 0, warped_tex = 0,
+                        ubefore_tex = 0, warp_tex = 0;
+  };
+  std::vector<Level> lv;
+  Plane<float> other0;
+  cudaTextureObject_t other0_tex = 0;
+  Plane<float2> calib;
+  Plane<float> smooth, warped;
+  Plane<float2> tvec;
+  TgvConsts cst;
+  float* cplanes[8];
+  TgvState st[2];
+  Plane<float> ubefore[2];
+  Plane<float2> warp[2];
+  float3* sched = nullptr;
+  int variant = 4;
+  bool mask_set = false, fields_set = false, solved = false;
+  std::vector<cudaTextureObject_t> textures;
+};
+
+namespace {
+
+int make_tex(VfsPlan* pl, const void* ptr, int h, int w, size_t pitch, int kind, int linear, cudaTextureObject_t* out) {
+  uint64_t t = 0;
+  int rc = vfs_texture_create(ptr, h, w, pitch, kind, linear, &t);
+  if (rc != VFS_OK) return rc;
+  *out = (cudaTextureObject_t)t;
+  pl->textures.push_back(*out);
+  return VFS_OK;
+}
+
+// Lays out (or, with base == nullptr, measures) every buffer of a plan.
+size_t layout(VfsPlan* pl, char* base) {
+  Carver cv{base};
+  const int L = pl->L;
+  for (int l = 0; l < L; ++l) {
+    auto& v = pl->lv[l];
+    v.ref = {cv.take<float>(pitch_of(v.w, 4) * v.h), pitch_of(v.w, 4)};
+    v.other = {cv.take<float>(pitch_of(v.w, 4) * v.h), pitch_of(v.w, 4)};
+    v.tvf = {cv.take<float2>(pitch_of(v.w, 8) * v.h), pitch_of(v.w, 8)};
+    v.mask = {cv.take<uint8_t>(pitch_of(v.w, 1) * v.h), pitch_of(v.w, 1)};
+    v.code = cv.take<uint8_t>((size_t)v.h * v.w);
+  }
+  const int h0 = pl->lv[0].h, w0 = pl->lv[0].w;
+  const size_t n0 = (size_t)h0 * w0;
+  pl->other0 = {cv.take<float>(pitch_of(w0, 4) * h0), pitch_of(w0, 4)};
+  pl->calib = {cv.take<float2>(n0 * 8), (size_t)w0 * 8};
+  pl->smooth = {cv.take<float>(pitch_of(w0, 4) * h0), pitch_of(w0, 4)};
+  pl->warped = {cv.take<float>(pitch_of(w0, 4) * h0), pitch_of(w0, 4)};
+  pl->tvec = {cv.take<float2>(n0 * 8), 0};
+  for (int i = 0; i < 8; ++i) pl->cplanes[i] = cv.take<float>(n0 * 4);
+  for (int b = 0; b < 2; ++b) {
+    float** f[10] = {&pl->st[b].u, &pl->st[b].ub, &pl->st[b].vbx, &pl->st[b].vby, &pl->st[b].px,
+                     &pl->st[b].py, &pl->st[b].qx, &pl->st[b].qy, &pl->st[b].qz, &pl->st[b].qw};
+    for (auto* pp : f) *pp = cv.take<float>(n0 * 4);
+    pl->ubefore[b] = {cv.take<float>(pitch_of(w0, 4) * h0), pitch_of(w0, 4)};
+    pl->warp[b] = {cv.take<float2>(pitch_of(w0, 8) * h0), pitch_of(w0, 8)};
+  }
+  pl->sched = cv.take<float3>(sizeof(float3) * std::max(1, pl->prm.nSolverIters));
+  pl->cst = {pl->cplanes[0], pl->cplanes[1], pl->cplanes[2], pl->cplanes[3], pl->cplanes[4],
+             pl->cplanes[5], pl->cplanes[6], pl->cplanes[7], nullptr};
+  return cv.off + kAlign;
+}
+
+void init_levels(VfsPlan* pl) {
+  pl->L = pl->prm.nLevel;
+  pl->lv.resize(pl->L);
+  // compute_pyramid_sizes, Python/vfs.py:84-91: int(prev / fScale)
+  int h = pl->prm.height, w = pl->prm.width;
+  for (int l = 0; l < pl->L; ++l) {
+    pl->lv[l].h = h;
+    pl->lv[l].w = w;
+    h = (int)(h / pl->prm.fScale);
+    w = (int)(w / pl->prm.fScale);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int vfs_plan_workspace_size(const VfsParams* prm, size_t* bytes) {
+  std::string why;
+  if (!valid_params(prm, &why)) return fail(VFS_ERR_ARG, why);
+  if (!bytes) return fail(VFS_ERR_ARG, "bytes is NULL");
+  VfsPlan tmp;
+  tmp.prm = *prm;
+  init_levels(&tmp);
+  for (auto& v : tmp.lv)
+    if (v.h <= 0 || v.w <= 0) return fail(VFS_ERR_ARG, "pyramid level has zero size; reduce nLevel");
+  *bytes = layout(&tmp, nullptr);
+  return VFS_OK;
+}
+
+int vfs_plan_create(const VfsParams* prm, void* workspace, size_t workspace_bytes, VfsPlan** plan_out) {
+  std::string why;
+  if (!valid_params(prm, &why)) return fail(VFS_ERR_ARG, why);
+  if (!plan_out) return fail(VFS_ERR_ARG, "plan_out is NULL");
+  size_t need = 0;
+  VFS_TRY(vfs_plan_workspace_size(prm, &need));
+  if (!workspace || workspace_bytes < need)
+    return fail(VFS_ERR_WORKSPACE, "workspace of " + std::to_string(need) + " bytes required");
+  VfsPlan* pl = new (std::nothrow) VfsPlan();
+  if (!pl) return fail(VFS_ERR_ARG, "out of host memory");
+  pl->prm = *prm;
+  pl->kc = make_consts(prm);
+  init_levels(pl);
+  char* base = reinterpret_cast<char*>(round_up(reinterpret_cast<uintptr_t>(workspace), kAlign));
+  layout(pl, base);
+  // step sizes, Python/vfs.py:494-515
+  std::vector<float> sched(3 * std::max(1, prm->nSolverIters), 0.f);
+  step_schedule(prm->nSolverIters, prm->timeStepLambda, sched.data());
+  cudaError_t e = cudaMemcpy(pl->sched, sched.data(), sched.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    delete pl;
+    return cuda_status(e, "schedule upload");
+  }
+  int rc = VFS_OK;
+  for (int l = 0; l < pl->L && rc == VFS_OK; ++l) {
+    auto& v = pl->lv[l];
+    if (rc == VFS_OK) rc = make_tex(pl, v.ref.ptr, v.h, v.w, v.ref.pitch, VFS_TEX_F32, 1, &v.ref_tex);
+    if (rc == VFS_OK) rc = make_tex(pl, v.other.ptr, v.h, v.w, v.other.pitch, VFS_TEX_F32, 1, &v.other_tex);
+    if (rc == VFS_OK) rc = make_tex(pl, v.tvf.ptr, v.h, v.w, v.tvf.pitch, VFS_TEX_F32X2, 1, &v.tvf_tex);
+    if (rc == VFS_OK) rc = make_tex(pl, v.mask.ptr, v.h, v.w, v.mask.pitch, VFS_TEX_U8, 0, &v.mask_tex);
+    if (rc == VFS_OK) rc = make_tex(pl, pl->smooth.ptr, v.h, v.w, pl->smooth.pitch, VFS_TEX_F32, 1, &v.smooth_tex);
+    if (rc == VFS_OK) rc = make_tex(pl, pl->warped.ptr, v.h, v.w, pl->warped.pitch, VFS_TEX_F32, 1, &v.warped_tex);
+    if (rc == VFS_OK)
+      rc = make_tex(pl, pl->ubefore[l % 2].ptr, v.h, v.w, pl->ubefore[l % 2].pitch, VFS_TEX_F32, 1, &v.ubefore_tex);
+    if (rc == VFS_OK)
+      rc = make_tex(pl, pl->warp[l % 2].ptr, v.h, v.w, pl->warp[l % 2].pitch, VFS_TEX_F32X2, 1, &v.warp_tex);
+  }
+  if (rc == VFS_OK)
+    rc = make_tex(pl, pl->other0.ptr, pl->lv[0].h, pl->lv[0].w, pl->other0.pitch, VFS_TEX_F32, 1, &pl->other0_tex);
+  if (rc != VFS_OK) {
+    vfs_plan_destroy(pl);
+    return rc;
+  }
+  *plan_out = pl;
+  return VFS_OK;
+}
+
+int vfs_plan_destroy(VfsPlan* pl) {
+  if (!pl) return VFS_OK;
+  for (auto t : pl->textures) cudaDestroyTextureObject(t);
+  delete pl;
+  return VFS_OK;
+}
+
+int vfs_plan_sizes(const VfsPlan* pl, int* hw) {
+  if (!pl || !hw) return fail(VFS_ERR_ARG, "NULL argument");
+  for (int l = 0; l < pl->L; ++l) {
+    hw[2 * l] = pl->lv[l].h;
+    hw[2 * l + 1] = pl->lv[l].w;
+  }
+  return VFS_OK;
+}
+
+int vfs_plan_set_tgv_variant(VfsPlan* pl, int k) {
+  if (!pl) return fail(VFS_ERR_ARG, "plan is NULL");
+  if (tgv_max_iters_per_launch(k) != k) return fail(VFS_ERR_ARG, "iterations per launch must be 1, 2 or 4");
+  pl->variant = k;
+  return VFS_OK;
+}
+
+int vfs_plan_set_mask(VfsPlan* pl, const uint8_t* mask, size_t mask_pitch, void* stream) {
+  if (!pl || !mask) return fail(VFS_ERR_ARG, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  auto& v0 = pl->lv[0];
+  if (mask_pitch == 0) mask_pitch = (size_t)v0.w;
+  VFS_TRY_CUDA(cudaMemcpy2DAsync(v0.mask.ptr, v0.mask.pitch, mask, mask_pitch, v0.w, v0.h, cudaMemcpyDeviceToDevice, s),
+               "mask copy");
+  // create_mask_pyramid, Python/vfs.py:159-187
+  for (int l = 1; l < pl->L; ++l) {
+    auto& v = pl->lv[l];
+    VFS_TRY_CUDA(launch_downsample_mask(v.mask, pl->lv[l - 1].mask_tex, v.h, v.w, s), "downSamplingMask");
+  }
+  pl->mask_set = true;
+  return VFS_OK;
+}
+
+int vfs_plan_set_vector_fields(VfsPlan* pl, const float* tvf, const float* cvf, void* stream) {
+  if (!pl || !tvf || !cvf) return fail(VFS_ERR_ARG, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  auto& v0 = pl->lv[0];
+  VFS_TRY_CUDA(cudaMemcpy2DAsync(v0.tvf.ptr, v0.tvf.pitch, tvf, (size_t)v0.w * 8, (size_t)v0.w * 8, v0.h,
+                                 cudaMemcpyDeviceToDevice, s),
+               "vector field copy");
+  VFS_TRY_CUDA(cudaMemcpyAsync(pl->calib.ptr, cvf, (size_t)v0.w * v0.h * 8, cudaMemcpyDeviceToDevice, s),
+               "calibration copy");
+  // create_vector_field_pyramid, Python/vfs.py:189-218
+  for (int l = 1; l < pl->L; ++l) {
+    auto& v = pl->lv[l];
+    VFS_TRY_CUDA(launch_downsample_field(v.tvf, pl->lv[l - 1].tvf_tex, v.h, v.w, s), "downSamplingVectorField");
+  }
+  pl->fields_set = true;
+  return VFS_OK;
+}
+
+int vfs_plan_solve(VfsPlan* pl, const uint8_t* img_ref, const uint8_t* img_other, float* warp_out, void* stream) {
+  if (!pl || !img_ref || !img_other || !warp_out) return fail(VFS_ERR_ARG, "NULL argument");
+  if (!pl->mask_set || !pl->fields_set)
+    return fail(VFS_ERR_STATE, "set_mask and set_vector_fields must precede solve");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int L = pl->L;
+  auto& v0 = pl->lv[0];
+  const SolverConsts& kc = pl->kc;
+  // create_image_pyramid, Python/vfs.py:121-157
+  VFS_TRY_CUDA(launch_cast_and_scale(v0.ref, {img_ref, (size_t)v0.w}, v0.h, v0.w, s), "castAndScale");
+  VFS_TRY_CUDA(launch_cast_and_scale(pl->other0, {img_other, (size_t)v0.w}, v0.h, v0.w, s), "castAndScale");
+  for (int l = 1; l < L; ++l)
+    VFS_TRY_CUDA(launch_downsample_image(pl->lv[l].ref, pl->lv[l - 1].ref_tex, pl->lv[l].h, pl->lv[l].w, s),
+                 "downSamplingImage");
+  VFS_TRY_CUDA(launch_warp_image(v0.other, {pl->calib.ptr, pl->calib.pitch}, pl->other0_tex, v0.h, v0.w, s),
+               "warpingImage");
+  for (int l = 1; l < L; ++l)
+    VFS_TRY_CUDA(launch_downsample_image(pl->lv[l].other, pl->lv[l - 1].other_tex, pl->lv[l].h, pl->lv[l].w, s),
+                 "downSamplingImage");
+
+  const int nIt = pl->prm.nSolverIters;
+  const int K = pl->variant;
+  const int npass = (nIt + K - 1) / K;
+  for (int l = L - 1; l >= 0; --l) {
+    auto& v = pl->lv[l];
+    const int h = v.h, w = v.w, b = l % 2;
+    const dim3 g = grid2d(h, w), blk(kBX, kBY);
+    if (l == L - 1) {  // warpUV, u, u_ <- 0 (Python/vfs.py:466-469)
+      VFS_TRY_CUDA(cudaMemset2DAsync(pl->ubefore[b].ptr, pl->ubefore[b].pitch, 0, (size_t)w * 4, h, s), "memset");
+      VFS_TRY_CUDA(cudaMemset2DAsync(pl->warp[b].ptr, pl->warp[b].pitch, 0, (size_t)w * 8, h, s), "memset");
+    }
+    Plane<const float> ub_src{pl->ubefore[b].ptr, pl->ubefore[b].pitch};
+    Plane<const uint8_t> mask{v.mask.ptr, v.mask.pitch};
+    // gaussian + computeTensorEtaMasked, Python/vfs.py:474-475
+    VFS_TRY_CUDA(launch_gaussian_masked(pl->smooth, v.ref_tex, mask, h, w, s), "gaussianMasked");
+    TgvConsts cst = pl->cst;
+    cst.code = v.code;
+    k_tensor_soa<<<g, blk, 0, s>>>(cst, v.code, v.smooth_tex, mask, kc, h, w);
+    VFS_TRY_CUDA(cudaGetLastError(), "tensor");
+    for (int wi = 0; wi < pl->prm.nWarpIters; ++wi) {
+      // findWarpingVector + warpingImage, Python/vfs.py:480-483
+      VFS_TRY_CUDA(launch_warp_prologue(Plane<float2>{pl->tvec.ptr, (size_t)w * 8}, pl->warped, {pl->warp[b].ptr, pl->warp[b].pitch}, v.tvf_tex, v.other_tex, h,
+                                        w, s),
+                   "warp prologue");
+      // computeDerivatives + solver reset, Python/vfs.py:486-497
+      k_derivs_init<<<g, blk, 0, s>>>(cst, pl->st[0], {pl->ubefore[b].ptr, pl->ubefore[b].pitch}, ub_src, v.ref_tex,
+                                      v.warped_tex, v.tvf_tex, h, w);
+      VFS_TRY_CUDA(cudaGetLastError(), "derivatives");
+      // solver iterations, Python/vfs.py:498-515
+      for (int j = 0; j < npass; ++j) {
+        const int it0 = j * K;
+        VFS_TRY_CUDA(launch_tgv_block(K, pl->st[j % 2], pl->st[(j + 1) % 2], cst, pl->sched, it0,
+                                      std::min(K, nIt - it0), kc, h, w, s),
+                     "tgv");
+      }
+      const TgvState& fin = pl->st[npass % 2];
+      // medianFilter + computeOpticalFlowWithClamp, Python/vfs.py:518-521
+      VFS_TRY_CUDA(launch_median_clamp({pl->warp[b].ptr, pl->warp[b].pitch}, pl->ubefore[b], {fin.u, (size_t)w * 4},
+                                       {pl->tvec.ptr, (size_t)w * 8}, mask, kc.upperLimit, h, w, s),
+                   "median/clamp");
+      ub_src = {fin.ub, (size_t)w * 4};
+    }
+    if (l > 0) {  // Python/vfs.py:523-528
+      auto& f = pl->lv[l - 1];
+      const int nb = (l - 1) % 2;
+      VFS_TRY_CUDA(launch_upsample1(pl->ubefore[nb], v.ubefore_tex, kc.fscale, f.h, f.w, s), "upSampling1");
+      VFS_TRY_CUDA(launch_upsample2(pl->warp[nb], v.warp_tex, kc.fscale, f.h, f.w, s), "upSampling");
+    }
+  }
+  // warpUV_ref[masks[0] == 0, :] = 0, Python/vfs.py:531
+  VFS_TRY_CUDA(launch_mask_flow(pl->warp[0], {v0.mask.ptr, v0.mask.pitch}, v0.h, v0.w, s), "mask flow");
+  VFS_TRY_CUDA(cudaMemcpy2DAsync(warp_out, (size_t)v0.w * 8, pl->warp[0].ptr, pl->warp[0].pitch, (size_t)v0.w * 8,
+                                 v0.h, cudaMemcpyDeviceToDevice, s),
+               "flow copy");
+  pl->solved = true;
+  return VFS_OK;
+}
+
+int vfs_plan_triangulate(VfsPlan* pl, float f, float u0, float v0f, const float* t, float* xyz_out, void* stream) {
+  if (!pl || !t || !xyz_out) return fail(VFS_ERR_ARG, "NULL argument");
+  if (!pl->solved) return fail(VFS_ERR_STATE, "triangulate needs a solve first");
+  auto& v0 = pl->lv[0];
+  VFS_TRY_CUDA(launch_triangulate_flow(reinterpret_cast<float3*>(xyz_out), {pl->warp[0].ptr, pl->warp[0].pitch},
+                                       Cam{f, u0, v0f}, t[0], t[1], t[2], {v0.mask.ptr, v0.mask.pitch}, v0.h, v0.w,
+                                       (cudaStream_t)stream),
+               "triangulate");
+  return VFS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,223 @@
+// Temporally blocked TGV-L1 primal-dual iterations (the solver loop of
+// Python/vfs.py:498-515: updateDualVariables -> l1Thresholding ->
+// updatePrimalVariables, Python/vfs.cu:326-581), fused into one kernel that
+// runs `k <= K` iterations per launch on a tile held in shared memory.
+//
+// Geometry.  One iteration at a pixel reads the previous state up to 2 pixels
+// towards W/N and 1 pixel towards E/S (the threshold and primal steps read
+// tp and q at the W and N neighbours, which the dual step forms from u_ and
+// v_ one pixel further out).  A CTA therefore loads its TX x TY tile plus a
+// halo of 2K pixels on the low sides and K on the high sides, iterates in
+// shared memory while the valid region shrinks by (2, 1) per iteration, and
+// writes back only the tile.  State is ping-ponged between two buffer sets
+// across launches, so a CTA never reads what a neighbour wrote in the same
+// launch.
+//
+// Flat addressing.  The reference reads data neighbours at flat offsets
+// index+-1 and index+-width (row-major, wrapping across rows at the image's
+// left and right edges), while it reads the mask in 2-D with edge clamping.
+// The window here maps window pixel (wx, wy) to flat index
+// (y0-2K+wy)*W + (x0-2K+wx), so every neighbour in the window is the flat
+// neighbour the reference reads, including the row wrap; the mask is carried
+// as a per-pixel code (self/E/W/S/N bits, computed in 2-D once per level)
+// addressed the same flat way.  Flat positions outside [0, H*W) hold zero
+// state and a zero code, which is what the reference's guarded reads see and
+// keeps them at zero.
+//
+// Per-pixel arithmetic is vfs_pixel.cuh's, shared with the one-kernel-per-
+// step entry points, so the fused solver is bit-identical to them.
+#include "vfs_tgv.cuh"
+
+namespace vfs {
+namespace {
+
+// Shared-memory planes (structure of arrays, one float per pixel each).
+enum SmemPlane {
+  sU, sUB, sVBX, sVBY, sPX, sPY, sQX, sQY, sQZ, sQW, sTPX, sTPY,
+  sA, sB, sC, sEX, sEY, sEZ, sIU, sIZ, kNumPlanes
+};
+
+template <int K, int TX, int TY>
+struct TgvGeom {
+  static constexpr int WX = TX + 3 * K;
+  static constexpr int WY = TY + 3 * K;
+  static constexpr int N = WX * WY;
+  static constexpr size_t smem_bytes() { return (size_t)kNumPlanes * N * sizeof(float) + ((N + 15) / 16) * 16; }
+};
+
+template <int K, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_tgv_block(TgvState in, TgvState out, TgvConsts cst,
+                                                  const float3* __restrict__ sched, int it0, int niter,
+                                                  SolverConsts kc, int h, int w) {
+  using G = TgvGeom<K, TX, TY>;
+  extern __shared__ float4 smem_raw[];
+  float* sm = reinterpret_cast<float*>(smem_raw);
+  uint8_t* scode = reinterpret_cast<uint8_t*>(sm + (size_t)kNumPlanes * G::N);
+  auto P = [&](int plane) { return sm + (size_t)plane * G::N; };
+
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const long n = (long)h * w;
+  const long base = (long)(y0 - 2 * K) * w + (x0 - 2 * K);
+
+  // ---- load the window (state, per-warp constants, mask code)
+  for (int e = threadIdx.x; e < G::N; e += NT) {
+    const int wy = e / G::WX, wx = e - wy * G::WX;
+    const long f = base + (long)wy * w + wx;
+    const bool ok = f >= 0 && f < n;
+    P(sU)[e] = ok ? in.u[f] : 0.f;
+    P(sUB)[e] = ok ? in.ub[f] : 0.f;
+    P(sVBX)[e] = ok ? in.vbx[f] : 0.f;
+    P(sVBY)[e] = ok ? in.vby[f] : 0.f;
+    P(sPX)[e] = ok ? in.px[f] : 0.f;
+    P(sPY)[e] = ok ? in.py[f] : 0.f;
+    P(sQX)[e] = ok ? in.qx[f] : 0.f;
+    P(sQY)[e] = ok ? in.qy[f] : 0.f;
+    P(sQZ)[e] = ok ? in.qz[f] : 0.f;
+    P(sQW)[e] = ok ? in.qw[f] : 0.f;
+    P(sA)[e] = ok ? cst.a[f] : 0.f;
+    P(sB)[e] = ok ? cst.b[f] : 0.f;
+    P(sC)[e] = ok ? cst.c[f] : 0.f;
+    P(sEX)[e] = ok ? cst.ex[f] : 0.f;
+    P(sEY)[e] = ok ? cst.ey[f] : 0.f;
+    P(sEZ)[e] = ok ? cst.ez[f] : 0.f;
+    P(sIU)[e] = ok ? cst.iu[f] : 0.f;
+    P(sIZ)[e] = ok ? cst.iz[f] : 0.f;
+    scode[e] = ok ? cst.code[f] : (uint8_t)0;
+  }
+  __syncthreads();
+
+  const int k = niter < K ? niter : K;
+  for (int s = 1; s <= k; ++s) {
+    const float3 ss = sched[it0 + s - 1];  // (sigma, tau, mu)
+    const float scaleP = kc.alpha1 * ss.x / kc.etaP;
+    const float scaleQ = kc.alpha0 * ss.x / kc.etaQ;
+    // dual step on [lo-1, hi) x [lo-1, hi), window coordinates
+    {
+      const int lo = 2 * K - 2 * (k - s) - 1;
+      const int hiX = 2 * K + TX + (k - s), hiY = 2 * K + TY + (k - s);
+      const int ex = hiX - lo, ey = hiY - lo;
+      for (int e = threadIdx.x; e < ex * ey; e += NT) {
+        const int ry = e / ex, rx = e - ry * ex;
+        const int i = (lo + ry) * G::WX + (lo + rx);
+        const uint8_t code = scode[i];
+        if (!(code & kSelf)) {
+          P(sPX)[i] = P(sPY)[i] = P(sTPX)[i] = P(sTPY)[i] = 0.f;
+          P(sQX)[i] = P(sQY)[i] = P(sQZ)[i] = P(sQW)[i] = 0.f;
+          continue;
+        }
+        float2 p = make_float2(P(sPX)[i], P(sPY)[i]), tp;
+        float4 q = make_float4(P(sQX)[i], P(sQY)[i], P(sQZ)[i], P(sQW)[i]);
+        const float* ub = P(sUB);
+        const float* vx = P(sVBX);
+        const float* vy = P(sVBY);
+        dual_px(code, ub[i], make_float2(vx[i], vy[i]), ub[i + 1], make_float2(vx[i + 1], vy[i + 1]), ub[i - 1],
+                make_float2(vx[i - 1], vy[i - 1]), ub[i + G::WX], make_float2(vx[i + G::WX], vy[i + G::WX]),
+                ub[i - G::WX], make_float2(vx[i - G::WX], vy[i - G::WX]),
+                make_float3(P(sA)[i], P(sB)[i], P(sC)[i]), scaleP, scaleQ, &p, &tp, &q);
+        P(sPX)[i] = p.x;
+        P(sPY)[i] = p.y;
+        P(sTPX)[i] = tp.x;
+        P(sTPY)[i] = tp.y;
+        P(sQX)[i] = q.x;
+        P(sQY)[i] = q.y;
+        P(sQZ)[i] = q.z;
+        P(sQW)[i] = q.w;
+      }
+    }
+    __syncthreads();
+    // threshold + primal steps on [lo, hi) x [lo, hi)
+    {
+      const int lo = 2 * K - 2 * (k - s);
+      const int hiX = 2 * K + TX + (k - s), hiY = 2 * K + TY + (k - s);
+      const int ex = hiX - lo, ey = hiY - lo;
+      for (int e = threadIdx.x; e < ex * ey; e += NT) {
+        const int ry = e / ex, rx = e - ry * ex;
+        const int i = (lo + ry) * G::WX + (lo + rx);
+        const uint8_t code = scode[i];
+        if (!(code & kSelf)) {
+          P(sU)[i] = P(sUB)[i] = P(sVBX)[i] = P(sVBY)[i] = 0.f;
+          continue;
+        }
+        const float u = P(sU)[i], ub = P(sUB)[i];
+        const float un = threshold_px(code, ss.y, make_float2(P(sTPX)[i], P(sTPY)[i]),
+                                      make_float2(P(sTPX)[i - 1], P(sTPY)[i - 1]),
+                                      make_float2(P(sTPX)[i - G::WX], P(sTPY)[i - G::WX]), u, ub,
+                                      make_float2(P(sIU)[i], P(sIZ)[i]), P(sEX)[i], kc.lambda);
+        float uo;
+        float2 vo;
+        primal_px(code, ss.y, ss.z, make_float2(P(sPX)[i], P(sPY)[i]),
+                  make_float4(P(sQX)[i], P(sQY)[i], P(sQZ)[i], P(sQW)[i]),
+                  make_float4(P(sQX)[i - 1], P(sQY)[i - 1], P(sQZ)[i - 1], P(sQW)[i - 1]),
+                  make_float4(P(sQX)[i - G::WX], P(sQY)[i - G::WX], P(sQZ)[i - G::WX], P(sQW)[i - G::WX]), un, ub,
+                  make_float2(P(sVBX)[i], P(sVBY)[i]), make_float3(P(sA)[i], P(sB)[i], P(sC)[i]),
+                  make_float3(P(sEX)[i], P(sEY)[i], P(sEZ)[i]), kc.alpha0, kc.alpha1, &uo, &vo);
+        P(sU)[i] = un;
+        P(sUB)[i] = uo;
+        P(sVBX)[i] = vo.x;
+        P(sVBY)[i] = vo.y;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- write back the tile (real pixels only)
+  for (int e = threadIdx.x; e < TX * TY; e += NT) {
+    const int ty = e / TX, tx = e - ty * TX;
+    const int X = x0 + tx, Y = y0 + ty;
+    if (X >= w || Y >= h) continue;
+    const int i = (2 * K + ty) * G::WX + (2 * K + tx);
+    const long f = (long)Y * w + X;
+    out.u[f] = P(sU)[i];
+    out.ub[f] = P(sUB)[i];
+    out.vbx[f] = P(sVBX)[i];
+    out.vby[f] = P(sVBY)[i];
+    out.px[f] = P(sPX)[i];
+    out.py[f] = P(sPY)[i];
+    out.qx[f] = P(sQX)[i];
+    out.qy[f] = P(sQY)[i];
+    out.qz[f] = P(sQZ)[i];
+    out.qw[f] = P(sQW)[i];
+  }
+}
+
+template <int K, int TX, int TY, int NT>
+cudaError_t launch_block(const TgvState& in, const TgvState& out, const TgvConsts& c, const float3* sched, int it0,
+                         int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
+  using G = TgvGeom<K, TX, TY>;
+  const size_t smem = G::smem_bytes();
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_tgv_block<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);
+  k_tgv_block<K, TX, TY, NT><<<grid, NT, smem, s>>>(in, out, c, sched, it0, niter, kc, h, w);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int tgv_max_iters_per_launch(int variant) {
+  switch (variant) {
+    case 1: return 1;
+    case 2: return 2;
+    case 4: return 4;
+    default: return 0;
+  }
+}
+
+cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& out, const TgvConsts& c,
+                             const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
+                             cudaStream_t s) {
+  if (h <= 0 || w <= 0 || niter <= 0) return cudaSuccess;
+  switch (variant) {
+    case 1: return launch_block<1, 32, 16, 256>(in, out, c, sched, it0, niter, kc, h, w, s);
+    case 2: return launch_block<2, 32, 32, 512>(in, out, c, sched, it0, niter, kc, h, w, s);
+    case 4: return launch_block<4, 32, 32, 512>(in, out, c, sched, it0, niter, kc, h, w, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace vfs

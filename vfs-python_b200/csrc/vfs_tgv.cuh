@@ -1,0 +1,36 @@
+// Fused TGV solver iterations: state and constant plane sets, launch entry.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "vfs_pixel.cuh"
+
+namespace vfs {
+
+// Solver state of one warp, structure of arrays, flat row-major planes of
+// h*w floats (row stride exactly w, as the reference's flat neighbour reads
+// assume).  u: thresholded flow increment; ub, vbx, vby: the over-relaxed
+// (bar) primal variables u_ and v_; p (2) and q (4): dual variables.
+struct TgvState {
+  float *u, *ub, *vbx, *vby, *px, *py, *qx, *qy, *qz, *qw;
+};
+
+// Per-warp constants, same flat layout: diffusion tensor (a, b, c), the
+// preconditioner eta (x, y, z), the image derivatives (iu, iz) and the mask
+// code (self/E/W/S/N bits).
+struct TgvConsts {
+  const float *a, *b, *c, *ex, *ey, *ez, *iu, *iz;
+  const uint8_t* code;
+};
+
+// Iterations per launch of each compiled variant (0 if unknown).
+int tgv_max_iters_per_launch(int variant);
+
+// Runs `niter` (<= the variant's K) iterations starting at schedule index
+// it0, reading `in` and writing `out` (distinct buffer sets).  `sched[i]` is
+// (sigma, tau, mu) of iteration i.
+cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& out, const TgvConsts& c,
+                             const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
+                             cudaStream_t s);
+
+}  // namespace vfs

@@ -1,0 +1,145 @@
+"""Seeded synthetic fisheye stereo pairs (the reference ships no benchmark data).
+
+A scene is a range field over the reference camera's pixels (a tilted plane
+plus eight Gaussian bumps, clipped to [1, 10] m) textured with 4-octave value
+noise in [0, 255] that is evaluated analytically at continuous coordinates.
+The second view sees every reference point ``X`` at ``X + t`` (no rotation),
+the convention of the reference's vector-field generator and triangulation
+(Python/vector_field.py:36-44, Python/vfs.cu:728-734).  For each pixel of the
+second image the reference pixel that lands there is found by fixed-point
+iteration on the flow, so the second image needs no resampling.
+
+The mask is the reference driver's circle (Python/main_equidistant.py:52-53)
+with margin ``max(10, 2**(nLevel-1))`` pixels.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def equidistant_intrinsics(width: int, height: int):
+    """180 degree field of view: f = (W/2)/(pi/2), principal point at the centre."""
+    return ((width / 2.0) / (math.pi / 2.0), width / 2.0, height / 2.0)
+
+
+def _project(X, f, cx, cy):
+    R = np.hypot(X[..., 0], X[..., 1])
+    th = np.arctan2(R, X[..., 2])
+    ph = np.arctan2(X[..., 1], X[..., 0])
+    return np.stack([f * th * np.cos(ph) + cx, f * th * np.sin(ph) + cy], -1)
+
+
+def _unproject(uv, f, cx, cy):
+    x = uv[..., 0] - cx
+    y = uv[..., 1] - cy
+    th = np.hypot(x, y) / f
+    ph = np.arctan2(y, x)
+    return np.stack([np.cos(ph) * np.sin(th), np.sin(ph) * np.sin(th), np.cos(th)], -1)
+
+
+class _ValueNoise:
+    def __init__(self, rng, width, height, octaves=4):
+        self.cells = [width / 16.0 / (2 ** o) for o in range(octaves)]
+        self.amps = [0.5 ** o for o in range(octaves)]
+        self.pad = 2.0 * max(width, height)
+        self.lat = []
+        for c in self.cells:
+            n = int(math.ceil((max(width, height) + 2 * self.pad) / c)) + 3
+            self.lat.append(rng.uniform(0.0, 1.0, (n, n)))
+
+    def __call__(self, x, y):
+        acc = np.zeros(np.shape(x))
+        for c, a, L in zip(self.cells, self.amps, self.lat):
+            gx = (np.asarray(x) + self.pad) / c
+            gy = (np.asarray(y) + self.pad) / c
+            gx = np.clip(gx, 0, L.shape[1] - 2.000001)
+            gy = np.clip(gy, 0, L.shape[0] - 2.000001)
+            ix = np.floor(gx).astype(np.int64)
+            iy = np.floor(gy).astype(np.int64)
+            fx = gx - ix
+            fy = gy - iy
+            sx = fx * fx * (3 - 2 * fx)
+            sy = fy * fy * (3 - 2 * fy)
+            v = ((1 - sx) * (1 - sy) * L[iy, ix] + sx * (1 - sy) * L[iy, ix + 1]
+                 + (1 - sx) * sy * L[iy + 1, ix] + sx * sy * L[iy + 1, ix + 1])
+            acc += a * v
+        return 255.0 * acc / sum(self.amps)
+
+
+class _Range:
+    def __init__(self, rng, width, height):
+        self.w, self.h = width, height
+        self.d0 = rng.uniform(3.0, 6.0)
+        self.gx = rng.uniform(-2.0, 2.0)
+        self.gy = rng.uniform(-2.0, 2.0)
+        self.bumps = []
+        for _ in range(8):
+            self.bumps.append((rng.uniform(0, width), rng.uniform(0, height),
+                               rng.uniform(width / 20.0, width / 8.0),
+                               rng.choice([-1.0, 1.0]) * rng.uniform(0.5, 2.0)))
+
+    def __call__(self, x, y):
+        d = self.d0 + self.gx * (x - self.w / 2) / self.w + self.gy * (y - self.h / 2) / self.h
+        for bx, by, s, a in self.bumps:
+            d = d + a * np.exp(-((x - bx) ** 2 + (y - by) ** 2) / (2 * s * s))
+        return np.clip(d, 1.0, 10.0)
+
+
+@dataclass
+class StereoPair:
+    img_ref: np.ndarray          # (H, W) uint8
+    img_other: np.ndarray        # (H, W) uint8
+    mask: np.ndarray             # (H, W) uint8, 255 = valid
+    intrinsics: tuple            # (f, u0, v0)
+    R: np.ndarray                # (3, 3)
+    t: np.ndarray                # (3, 1)
+    depth: np.ndarray            # (H, W) float32 z-depth of the reference view
+    seed: int = 0
+    meta: dict = field(default_factory=dict)
+
+
+def circle_mask(height: int, width: int, margin: int) -> np.ndarray:
+    """Filled circle centred at (W//2, H//2) with radius W//2 - margin, as
+    ``cv2.circle(mask, (W//2, H//2), W//2 - margin, 255, -1)``."""
+    import cv2
+    mask = np.zeros((height, width), np.uint8)
+    cv2.circle(mask, (width // 2, height // 2), width // 2 - margin, 255, -1)
+    return mask
+
+
+def make_pair(size: int, t, seed: int = 0, n_level: int = 4, height: int | None = None) -> StereoPair:
+    """One seeded pair at ``size`` x ``size`` (or ``height`` x ``size``)."""
+    W = int(size)
+    H = int(height if height is not None else size)
+    t = np.asarray(t, np.float64).reshape(3)
+    rng = np.random.default_rng(seed)
+    f, cx, cy = equidistant_intrinsics(W, H)
+    noise = _ValueNoise(rng, W, H)
+    rng_field = _Range(rng, W, H)
+
+    yy, xx = np.meshgrid(np.arange(H, dtype=np.float64), np.arange(W, dtype=np.float64), indexing="ij")
+    img_ref = noise(xx, yy)
+
+    def flow(px, py):
+        ray = _unproject(np.stack([px, py], -1), f, cx, cy)
+        X = rng_field(px, py)[..., None] * ray + t
+        uv = _project(X, f, cx, cy)
+        return uv[..., 0] - px, uv[..., 1] - py
+
+    p1x, p1y = xx.copy(), yy.copy()
+    for _ in range(30):
+        fx, fy = flow(p1x, p1y)
+        p1x = 0.5 * p1x + 0.5 * (xx - fx)
+        p1y = 0.5 * p1y + 0.5 * (yy - fy)
+    img_other = noise(p1x, p1y)
+
+    ray = _unproject(np.stack([xx, yy], -1), f, cx, cy)
+    depth = (rng_field(xx, yy) * ray[..., 2]).astype(np.float32)
+    margin = max(10, 2 ** (n_level - 1))
+    mask = circle_mask(H, W, margin)
+    q = lambda a: np.clip(np.round(a), 0, 255).astype(np.uint8)
+    return StereoPair(q(img_ref), q(img_other), mask, (f, cx, cy), np.eye(3), t.reshape(3, 1), depth, seed,
+                      {"margin": margin})
