@@ -1,0 +1,426 @@
+"""Benchmark: depth maps/s of the variational fisheye stereo solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one step = one depth map): an 800x800 equidistant fisheye pair
+(f = 400/(pi/2), principal point at the centre, t = (0.12, 0.01, 0) m, no
+rotation), 5-level pyramid at scale 0.5, 10 warps per level, 100 TGV
+iterations, lambda 50, alpha0 17, alpha1 1.2, beta 9, gamma 0.85, float32;
+solve_stereo followed by triangulate_flow.  The pair is synthetic (seeded
+range field + value-noise texture, see vfs_b200/synthetic.py): the reference
+publishes no benchmark data.
+
+``value``: device time of K steps with inputs resident in HBM (CUDA events on
+the solve's stream; L2 is flushed by writing 256 MiB between steps, outside
+the timed events).  ``e2e``: the same through the public Python API from
+pinned host images, with the host->device copy of both images and the
+device->host copy of the depth map inside the timed region.  With N > 1 GPUs
+each rank solves its own pair (weak scaling, no collective on the data path);
+times are the max over ranks.
+
+``--impl reference``: the reference's own CUDA kernels (built from its sources
+into oracle/_ref) under the reference's host loop, which launches one kernel
+per step and synchronises the device after each, on the same pair; rank 0
+only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "vfs-python_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "depth maps/s at 800² fused-batched vs plain on one B200 @≤1e-4 err; fwd+bwd/s"
+UNIT = "depth maps/s"
+SIZE = 800
+T = (0.12, 0.01, 0.0)
+N_LEVEL, N_WARP, N_ITER = 5, 10, 100
+ALG_BYTES_ITER, ALG_BYTES_WARP, ALG_BYTES_LEVEL = 113, 60, 41
+
+
+def params():
+    from vfs_b200.vfs_params import vfs_params
+    p = vfs_params()
+    p.width = p.height = SIZE
+    p.nLevel, p.fScale, p.nWarpIters, p.nSolverIters = N_LEVEL, 2.0, N_WARP, N_ITER
+    p.Lambda, p.alpha0, p.alpha1, p.beta, p.gamma = 50.0, 17.0, 1.2, 9.0, 0.85
+    p.timeStepLambda, p.limitRange = 1.0, 0.1
+    return p
+
+
+def level_pixels(p):
+    out, h, w = [], p.height, p.width
+    for _ in range(p.nLevel):
+        out.append(h * w)
+        h, w = int(h / p.fScale), int(w / p.fScale)
+    return out
+
+
+def alg_bytes_per_map(p):
+    return sum(n * (p.nWarpIters * (p.nSolverIters * ALG_BYTES_ITER + ALG_BYTES_WARP) + ALG_BYTES_LEVEL)
+               for n in level_pixels(p))
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for n, v in zip(names, r[4:8]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    n = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if n > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    return n, rank, local
+
+
+def max_over_ranks(x: float, n: int) -> float:
+    if n == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(n):
+    if n > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+
+def make_inputs(seed):
+    from vfs_b200.synthetic import make_pair
+    return make_pair(SIZE, T, seed=seed, n_level=N_LEVEL)
+
+
+def setup_b200(pair, p):
+    from vfs_b200 import VFS, EquidistantCam
+    from vfs_b200.vector_field import get_vector_fields, get_grid_zero
+    cam = EquidistantCam(pair.intrinsics)
+    cam.setup_module()
+    tvf, cvf = get_vector_fields(get_grid_zero(pair.img_ref.shape), cam, cam, pair.R, pair.t, 1)
+    vfs = VFS(p)
+    vfs.setup_module()
+    vfs.compute_pyramid_sizes()
+    vfs.create_mask_pyramid(pair.mask)
+    vfs.create_vector_field_pyramid(tvf, cvf)
+    return vfs, cam
+
+
+def cpu_baseline_sample(pair, p, budget_s=20.0):
+    """float64 NumPy oracle on the host, one core: the finest level's
+    per-level and per-warp work plus a few TGV iterations, extrapolated to a
+    full depth map by pixel-iteration counts."""
+    from oracle.np64 import vfs64 as V
+    cam = V.EquidistantCam64(pair.intrinsics)
+    tvf, cvf = V.get_vector_fields(V.get_grid_zero(pair.img_ref.shape), cam, cam, pair.R, pair.t, 1)
+    v = V.VFS64(p)
+    v.compute_pyramid_sizes()
+    v.create_mask_pyramid(pair.mask)
+    v.create_vector_field_pyramid(tvf, cvf)
+    v.create_image_pyramid(pair.img_ref, pair.img_other)
+    M = v.masks[0]
+    s = v.sizes[0]
+    t0 = time.perf_counter()
+    sm = V.gaussian_masked(v.refs[0], M)
+    abc, eta = V.compute_tensor_eta(sm, M, p)
+    t_level = time.perf_counter() - t0
+    warp = np.zeros((*s, 2))
+    u = np.zeros(s)
+    u_ = np.zeros(s)
+    t0 = time.perf_counter()
+    tvec = V.find_warping_vector(v.translations[0], warp)
+    warped = V.warping_image(v.others[0], warp)
+    deriv = V.compute_derivatives(v.refs[0], warped, v.translations[0])
+    t_warp = time.perf_counter() - t0
+    p_ = np.zeros((*s, 2))
+    q = np.zeros((*s, 4))
+    vb = np.zeros((*s, 2))
+    ub4 = u.copy()
+    sched = V.step_schedule(p.nSolverIters, p.timeStepLambda)
+    n_it = 0
+    t0 = time.perf_counter()
+    for sigma, tau, mu in sched:
+        p_, tp, q = V.update_dual_variables(p_, q, sigma, u_, vb, abc, M, p)
+        u = V.l1_thresholding(tau, tp, u, u_, deriv, eta, M, p)
+        u_, vb = V.update_primal_variables(tau, mu, p_, q, u, u_, vb, abc, eta, M, p)
+        n_it += 1
+        if time.perf_counter() - t0 > budget_s or n_it >= 20:
+            break
+    t_iter = (time.perf_counter() - t0) / n_it
+    t1 = time.perf_counter()
+    med = V.median_filter(u, M)
+    V.compute_optical_flow_with_clamp(warp, ub4, med, tvec, M, p)
+    t_warp += time.perf_counter() - t1
+    n0 = s[0] * s[1]
+    per_px = lambda t: t / n0
+    t_map = sum(n * (p.nWarpIters * (p.nSolverIters * per_px(t_iter) + per_px(t_warp)) + per_px(t_level))
+                for n in level_pixels(p))
+    return {"value": 1.0 / t_map, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"float64 NumPy oracle at 800x800: per-level + per-warp work once and {n_it} TGV iterations "
+                      f"({t_iter:.2f} s each), extrapolated by pixel-iterations to 5 levels x 10 warps x 100 "
+                      f"iterations ({t_map:.0f} s per map)"}
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "k_tgv_block_800x800_ncu.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def run_b200(args, n, rank, local):
+    p = params()
+    pair = make_inputs(seed=rank)
+    vfs, cam = setup_b200(pair, p)
+    vfs.configure(iters_per_launch=args.iters_per_launch, use_graph=not args.no_graph, timing=True)
+    ref_d = torch.as_tensor(pair.img_ref).cuda()
+    oth_d = torch.as_tensor(pair.img_other).cuda()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        vfs.solve_stereo(ref_d, oth_d)
+        return vfs.triangulate_flow(cam, pair.t)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    kernels = vfs.solve_stats()["kernels_per_solve"] + 1
+
+    # ---- device-resident throughput
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    tgv_ms = tgv_bytes = 0.0
+    tgv_launches = 0
+    barrier(n)
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+            st = vfs.solve_stats()  # synchronises
+            tgv_ms += st["tgv_ms"]
+            tgv_bytes += st["tgv_alg_bytes"]
+            tgv_launches += st["tgv_launches"]
+    barrier(n)
+    elapsed = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+    t_max = max_over_ranks(elapsed, n)
+    value = n * args.steps / t_max
+
+    # ---- end to end through the public API from pinned host memory
+    h_ref = torch.as_tensor(pair.img_ref).pin_memory()
+    h_oth = torch.as_tensor(pair.img_other).pin_memory()
+    h_depth = torch.empty((SIZE, SIZE), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        d_ref = h_ref.to("cuda", non_blocking=True)
+        d_oth = h_oth.to("cuda", non_blocking=True)
+        vfs.solve_stereo(d_ref, d_oth)
+        xyz = vfs.triangulate_flow(cam, pair.t)
+        h_depth.copy_(xyz[:, :, 2], non_blocking=True)
+
+    vfs.configure(timing=False)
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier(n)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        ev2[i][0].record(stream)
+        e2e_step()
+        ev2[i][1].record(stream)
+        ev2[i][1].synchronize()
+    barrier(n)
+    e2e_t = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev2) / 1e3, n)
+    e2e_value = n * args.steps / e2e_t
+    depth = h_depth.numpy()
+    m = (pair.mask > 0) & (pair.depth > 0)
+
+    peak, peak_kind = measured_peak()
+    achieved = tgv_bytes / (tgv_ms / 1e3) / 1e9 if tgv_ms > 0 else None
+    traffic = None
+    tr = load_traffic()
+    if tr and tgv_launches:
+        traffic = tr["dram_bytes_per_alg_byte"] * (tgv_bytes / tgv_launches)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded range field + value-noise texture, 800x800 fisheye pair per rank)",
+        "config": {"workload": "800x800 equidistant fisheye pair, 5 levels x 10 warps x 100 TGV iterations, "
+                               "solve_stereo + triangulate_flow",
+                   "size": SIZE, "levels": N_LEVEL, "warps": N_WARP, "iterations": N_ITER, "lambda": 50.0,
+                   "t": list(T), "tgv_iters_per_launch": args.iters_per_launch, "cuda_graph": not args.no_graph,
+                   "l2": "flushed between steps (256 MiB write outside the timed events)",
+                   "parallelism": f"dp{n} (independent pairs)"},
+        "roofline": {"bound": "hbm", "kernel": "k_tgv_block (fused TGV iterations)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                     "traffic": traffic,
+                     "alg_bytes_per_launch": tgv_bytes / max(tgv_launches, 1),
+                     "avg_launch_us": 1e3 * tgv_ms / max(tgv_launches, 1),
+                     "tgv_share_of_step": (tgv_ms / 1e3) / elapsed if elapsed else None},
+        "alg_bytes_per_map": alg_bytes_per_map(p),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * SIZE * SIZE,
+                "d2h_bytes_per_step": 4 * SIZE * SIZE},
+        "gpu_launches": int(kernels * args.steps),
+        "clocks": clk.summary(),
+        "depth_check": {"median_rel_err_vs_ground_truth": float(np.median(
+            np.abs(depth[m] - pair.depth[m]) / pair.depth[m]))},
+    }
+    if n == 1 and rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(pair, p, budget_s=args.cpu_budget)
+    return line
+
+
+def run_reference(args, n, rank, local):
+    from oracle.refgpu import refpath
+    p = params()
+    pair = make_inputs(seed=0)
+    from oracle.np64 import vfs64 as V
+    cam64 = V.EquidistantCam64(pair.intrinsics)
+    tvf, cvf = V.get_vector_fields(V.get_grid_zero(pair.img_ref.shape), cam64, cam64, pair.R, pair.t, 1)
+    tvf, cvf = tvf.astype(np.float32), cvf.astype(np.float32)
+    r = refpath.RefVFS(p, "bench")
+    r.compute_pyramid_sizes()
+    r.create_mask_pyramid(pair.mask)
+    r.create_vector_field_pyramid(tvf, cvf)
+    cam = refpath.RefEquidistantCam(pair.intrinsics, "bench")
+    cam.setup_module()
+
+    def step():
+        r.solve_stereo(pair.img_ref, pair.img_other)
+        return r.triangulate_flow(cam, pair.t)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    value = args.steps / el
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "impl": "reference", "data": "synthetic (same pair as the b200 arm, seed 0)",
+        "config": {"workload": "800x800 equidistant fisheye pair, 5 levels x 10 warps x 100 TGV iterations, "
+                               "solve_stereo + triangulate_flow",
+                   "size": SIZE, "levels": N_LEVEL, "warps": N_WARP, "iterations": N_ITER, "lambda": 50.0,
+                   "t": list(T), "parallelism": "single GPU",
+                   "l2": "not flushed (the reference's host loop synchronises after every launch)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"{args.steps} full 800x800 solves: the reference's CUDA kernels on the B200, "
+                                   "launched and synchronised one at a time by one host thread"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.perf_counter() - t0,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--iters-per-launch", type=int, default=4)
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 1)
+    n, rank, local = dist_init()
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, n, rank, local)), flush=True)
+    else:
+        line = run_b200(args, n, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    if n > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -162,7 +162,24 @@ VFS_API int vfs_plan_triangulate(VfsPlan* plan, float f, float u0, float v0, con
  * reference's host loop computes them (Python/vfs.py:494-515, NumPy >= 2
  * scalar rules); out3 receives 3*n floats.  Host-only, no GPU needed. */
 VFS_API int vfs_step_schedule(int n, double time_step_lambda, float* out3);
-/* Select the fused TGV variant (iterations per launch: 1, 2 or 4). */
+/* Replay the whole solve as one CUDA graph (captured on the first solve after
+ * enabling, on a stream the plan owns, ordered after `stream`). */
+VFS_API int vfs_plan_set_graph(VfsPlan* plan, int enable);
+/* Record an event pair around each warp's TGV launches (for measurement). */
+VFS_API int vfs_plan_set_timing(VfsPlan* plan, int enable);
+typedef struct VfsSolveStats {
+  long long kernels_per_solve; /* kernels one solve launches */
+  double tgv_ms;               /* summed device time of the TGV launches (timing on) */
+  double tgv_alg_bytes;        /* their algorithmic bytes: 113 per pixel-iteration */
+  long long tgv_launches;      /* number of TGV kernel launches timed */
+  int tgv_intervals;           /* event pairs summed */
+} VfsSolveStats;
+/* Statistics of the last solve; synchronise its stream first. */
+VFS_API int vfs_plan_stats(VfsPlan* plan, VfsSolveStats* out);
+/* Compiled fused-TGV kernel variants: returns their number and writes up to
+ * `cap` ids and their iterations per launch. */
+VFS_API int vfs_tgv_variants(int* ids, int cap, int* iters_per_launch);
+/* Select the fused TGV kernel variant by id (see vfs_tgv_variants). */
 VFS_API int vfs_plan_set_tgv_variant(VfsPlan* plan, int iters_per_launch);
 
 #ifdef __cplusplus

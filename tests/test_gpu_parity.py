@@ -178,7 +178,10 @@ def _solve_pair(ref_mod, prm, p, lib_name=None, mask=None, variants=(4,)):
     for v in variants:
         o.tgv_iters_per_launch = v
         o.release()
-        ow = _np(o.solve_stereo(p.img_ref, p.img_other))
+        try:
+            ow = _np(o.solve_stereo(p.img_ref, p.img_other))
+        except Exception as e:
+            raise AssertionError(f"TGV variant {v}: {e}") from e
         oxyz = _np(o.triangulate_flow(cam, p.t))
         outs[v] = (ow, oxyz)
     return (rw, rxyz), outs, o, cam
@@ -189,7 +192,11 @@ def test_solve_bit_exact_bench_params(ref_mod, n_iter):
     h, w = 96, 128
     p = pair(w, height=h, t=(0.12, 0.01, 0.0), seed=1, n_level=3)
     prm = bench_params(h, w, n_level=3, n_warp=3, n_iter=n_iter)
-    (rw, rxyz), outs, o, cam = _solve_pair(ref_mod, prm, p, variants=(1, 2, 4))
+    from vfs_b200 import _lib
+    import ctypes
+    ids = (ctypes.c_int * 64)()
+    n = _lib.lib().vfs_tgv_variants(ids, 64, None)
+    (rw, rxyz), outs, o, cam = _solve_pair(ref_mod, prm, p, variants=tuple(ids[i] for i in range(n)))
     for v, (ow, oxyz) in outs.items():
         assert_bits_equal(rw, ow, f"warpUV (iterations per launch {v})")
         assert_bits_equal(rxyz, oxyz, f"xyz (iterations per launch {v})")

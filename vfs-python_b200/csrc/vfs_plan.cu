@@ -111,6 +111,26 @@ struct VfsPlan {
   int variant = 4;
   bool mask_set = false, fields_set = false, solved = false;
   std::vector<cudaTextureObject_t> textures;
+  // input staging (workspace), so a captured graph has fixed pointers
+  uint8_t* stage_ref = nullptr;
+  uint8_t* stage_other = nullptr;
+  // graph replay
+  bool use_graph = false;
+  cudaStream_t gstream = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // instrumentation: an event pair around each warp's TGV launches
+  bool timing = false;
+  std::vector<cudaEvent_t> tev;
+  std::vector<double> tev_bytes;
+  std::vector<long long> tev_launches;
+  int tev_used = 0;
+  long long kernels_per_solve = 0;
+
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+  }
 };
 
 namespace {
@@ -152,6 +172,8 @@ size_t layout(VfsPlan* pl, char* base) {
     pl->warp[b] = {cv.take<float2>(pitch_of(w0, 8) * h0), pitch_of(w0, 8)};
   }
   pl->sched = cv.take<float3>(sizeof(float3) * std::max(1, pl->prm.nSolverIters));
+  pl->stage_ref = cv.take<uint8_t>(n0);
+  pl->stage_other = cv.take<uint8_t>(n0);
   pl->cst = {pl->cplanes[0], pl->cplanes[1], pl->cplanes[2], pl->cplanes[3], pl->cplanes[4],
              pl->cplanes[5], pl->cplanes[6], pl->cplanes[7], nullptr};
   return cv.off + kAlign;
@@ -168,6 +190,110 @@ void init_levels(VfsPlan* pl) {
     h = (int)(h / pl->prm.fScale);
     w = (int)(w / pl->prm.fScale);
   }
+}
+
+// Enqueues one complete solve on `s` from the staged images into warp[0].
+int enqueue_solve(VfsPlan* pl, cudaStream_t s) {
+  const int L = pl->L;
+  auto& v0 = pl->lv[0];
+  const SolverConsts& kc = pl->kc;
+  long long nk = 0;
+  pl->tev_used = 0;
+  // create_image_pyramid, Python/vfs.py:121-157
+  VFS_TRY_CUDA(launch_cast_and_scale(v0.ref, {pl->stage_ref, (size_t)v0.w}, v0.h, v0.w, s), "castAndScale");
+  VFS_TRY_CUDA(launch_cast_and_scale(pl->other0, {pl->stage_other, (size_t)v0.w}, v0.h, v0.w, s), "castAndScale");
+  nk += 2;
+  for (int l = 1; l < L; ++l, ++nk)
+    VFS_TRY_CUDA(launch_downsample_image(pl->lv[l].ref, pl->lv[l - 1].ref_tex, pl->lv[l].h, pl->lv[l].w, s),
+                 "downSamplingImage");
+  VFS_TRY_CUDA(launch_warp_image(v0.other, {pl->calib.ptr, pl->calib.pitch}, pl->other0_tex, v0.h, v0.w, s),
+               "warpingImage");
+  ++nk;
+  for (int l = 1; l < L; ++l, ++nk)
+    VFS_TRY_CUDA(launch_downsample_image(pl->lv[l].other, pl->lv[l - 1].other_tex, pl->lv[l].h, pl->lv[l].w, s),
+                 "downSamplingImage");
+
+  const int nIt = pl->prm.nSolverIters;
+  const int K = tgv_max_iters_per_launch(pl->variant);
+  const int npass = (nIt + K - 1) / K;
+  for (int l = L - 1; l >= 0; --l) {
+    auto& v = pl->lv[l];
+    const int h = v.h, w = v.w, b = l % 2;
+    const dim3 g = grid2d(h, w), blk(kBX, kBY);
+    if (l == L - 1) {  // warpUV, u, u_ <- 0 (Python/vfs.py:466-469)
+      VFS_TRY_CUDA(cudaMemset2DAsync(pl->ubefore[b].ptr, pl->ubefore[b].pitch, 0, (size_t)w * 4, h, s), "memset");
+      VFS_TRY_CUDA(cudaMemset2DAsync(pl->warp[b].ptr, pl->warp[b].pitch, 0, (size_t)w * 8, h, s), "memset");
+    }
+    Plane<const float> ub_src{pl->ubefore[b].ptr, pl->ubefore[b].pitch};
+    Plane<const uint8_t> mask{v.mask.ptr, v.mask.pitch};
+    // gaussian + computeTensorEtaMasked, Python/vfs.py:474-475
+    VFS_TRY_CUDA(launch_gaussian_masked(pl->smooth, v.ref_tex, mask, h, w, s), "gaussianMasked");
+    TgvConsts cst = pl->cst;
+    cst.code = v.code;
+    k_tensor_soa<<<g, blk, 0, s>>>(cst, v.code, v.smooth_tex, mask, kc, h, w);
+    VFS_TRY_CUDA(cudaGetLastError(), "tensor");
+    nk += 2;
+    for (int wi = 0; wi < pl->prm.nWarpIters; ++wi) {
+      // findWarpingVector + warpingImage, Python/vfs.py:480-483
+      VFS_TRY_CUDA(launch_warp_prologue(Plane<float2>{pl->tvec.ptr, (size_t)w * 8}, pl->warped,
+                                        {pl->warp[b].ptr, pl->warp[b].pitch}, v.tvf_tex, v.other_tex, h, w, s),
+                   "warp prologue");
+      // computeDerivatives + solver reset, Python/vfs.py:486-497
+      k_derivs_init<<<g, blk, 0, s>>>(cst, pl->st[0], {pl->ubefore[b].ptr, pl->ubefore[b].pitch}, ub_src, v.ref_tex,
+                                      v.warped_tex, v.tvf_tex, h, w);
+      VFS_TRY_CUDA(cudaGetLastError(), "derivatives");
+      nk += 2;
+      // solver iterations, Python/vfs.py:498-515
+      const bool timed = pl->timing && npass > 0;
+      if (timed) {
+        const int pair = pl->tev_used;
+        while ((int)pl->tev.size() < 2 * (pair + 1)) {
+          cudaEvent_t e;
+          VFS_TRY_CUDA(cudaEventCreate(&e), "event create");
+          pl->tev.push_back(e);
+        }
+        if ((int)pl->tev_bytes.size() < pair + 1) {
+          pl->tev_bytes.resize(pair + 1);
+          pl->tev_launches.resize(pair + 1);
+        }
+        VFS_TRY_CUDA(cudaEventRecordWithFlags(pl->tev[2 * pair], s, cudaEventRecordExternal), "event record");
+      }
+      for (int j = 0; j < npass; ++j) {
+        const int it0 = j * K;
+        VFS_TRY_CUDA(launch_tgv_block(pl->variant, pl->st[j % 2], pl->st[(j + 1) % 2], cst, pl->sched, it0,
+                                      std::min(K, nIt - it0), kc, h, w, s),
+                     "tgv");
+      }
+      nk += npass;
+      if (timed) {
+        const int pair = pl->tev_used++;
+        VFS_TRY_CUDA(cudaEventRecordWithFlags(pl->tev[2 * pair + 1], s, cudaEventRecordExternal), "event record");
+        // algorithmic bytes: 113 per pixel per iteration (state in and out,
+        // per-warp constants in)
+        pl->tev_bytes[pair] = 113.0 * (double)h * w * nIt;
+        pl->tev_launches[pair] = npass;
+      }
+      const TgvState& fin = pl->st[npass % 2];
+      // medianFilter + computeOpticalFlowWithClamp, Python/vfs.py:518-521
+      VFS_TRY_CUDA(launch_median_clamp({pl->warp[b].ptr, pl->warp[b].pitch}, pl->ubefore[b], {fin.u, (size_t)w * 4},
+                                       {pl->tvec.ptr, (size_t)w * 8}, mask, kc.upperLimit, h, w, s),
+                   "median/clamp");
+      ++nk;
+      ub_src = {fin.ub, (size_t)w * 4};
+    }
+    if (l > 0) {  // Python/vfs.py:523-528
+      auto& f = pl->lv[l - 1];
+      const int nb = (l - 1) % 2;
+      VFS_TRY_CUDA(launch_upsample1(pl->ubefore[nb], v.ubefore_tex, kc.fscale, f.h, f.w, s), "upSampling1");
+      VFS_TRY_CUDA(launch_upsample2(pl->warp[nb], v.warp_tex, kc.fscale, f.h, f.w, s), "upSampling");
+      nk += 2;
+    }
+  }
+  // warpUV_ref[masks[0] == 0, :] = 0, Python/vfs.py:531
+  VFS_TRY_CUDA(launch_mask_flow(pl->warp[0], {v0.mask.ptr, v0.mask.pitch}, v0.h, v0.w, s), "mask flow");
+  ++nk;
+  pl->kernels_per_solve = nk;
+  return VFS_OK;
 }
 
 }  // namespace
@@ -224,6 +350,7 @@ int vfs_plan_create(const VfsParams* prm, void* workspace, size_t workspace_byte
     if (rc == VFS_OK)
       rc = make_tex(pl, pl->warp[l % 2].ptr, v.h, v.w, pl->warp[l % 2].pitch, VFS_TEX_F32X2, 1, &v.warp_tex);
   }
+  if (rc == VFS_OK) rc = cuda_status(tgv_prepare(), "tgv kernel attributes");
   if (rc == VFS_OK)
     rc = make_tex(pl, pl->other0.ptr, pl->lv[0].h, pl->lv[0].w, pl->other0.pitch, VFS_TEX_F32, 1, &pl->other0_tex);
   if (rc != VFS_OK) {
@@ -237,6 +364,11 @@ int vfs_plan_create(const VfsParams* prm, void* workspace, size_t workspace_byte
 int vfs_plan_destroy(VfsPlan* pl) {
   if (!pl) return VFS_OK;
   for (auto t : pl->textures) cudaDestroyTextureObject(t);
+  pl->drop_graph();
+  if (pl->gstream) cudaStreamDestroy(pl->gstream);
+  if (pl->ev_in) cudaEventDestroy(pl->ev_in);
+  if (pl->ev_out) cudaEventDestroy(pl->ev_out);
+  for (auto e : pl->tev) cudaEventDestroy(e);
   delete pl;
   return VFS_OK;
 }
@@ -252,7 +384,7 @@ int vfs_plan_sizes(const VfsPlan* pl, int* hw) {
 
 int vfs_plan_set_tgv_variant(VfsPlan* pl, int k) {
   if (!pl) return fail(VFS_ERR_ARG, "plan is NULL");
-  if (tgv_max_iters_per_launch(k) != k) return fail(VFS_ERR_ARG, "iterations per launch must be 1, 2 or 4");
+  if (tgv_max_iters_per_launch(k) == 0) return fail(VFS_ERR_ARG, "unknown TGV kernel variant");
   pl->variant = k;
   return VFS_OK;
 }
@@ -296,76 +428,85 @@ int vfs_plan_solve(VfsPlan* pl, const uint8_t* img_ref, const uint8_t* img_other
   if (!pl->mask_set || !pl->fields_set)
     return fail(VFS_ERR_STATE, "set_mask and set_vector_fields must precede solve");
   cudaStream_t s = (cudaStream_t)stream;
-  const int L = pl->L;
   auto& v0 = pl->lv[0];
-  const SolverConsts& kc = pl->kc;
-  // create_image_pyramid, Python/vfs.py:121-157
-  VFS_TRY_CUDA(launch_cast_and_scale(v0.ref, {img_ref, (size_t)v0.w}, v0.h, v0.w, s), "castAndScale");
-  VFS_TRY_CUDA(launch_cast_and_scale(pl->other0, {img_other, (size_t)v0.w}, v0.h, v0.w, s), "castAndScale");
-  for (int l = 1; l < L; ++l)
-    VFS_TRY_CUDA(launch_downsample_image(pl->lv[l].ref, pl->lv[l - 1].ref_tex, pl->lv[l].h, pl->lv[l].w, s),
-                 "downSamplingImage");
-  VFS_TRY_CUDA(launch_warp_image(v0.other, {pl->calib.ptr, pl->calib.pitch}, pl->other0_tex, v0.h, v0.w, s),
-               "warpingImage");
-  for (int l = 1; l < L; ++l)
-    VFS_TRY_CUDA(launch_downsample_image(pl->lv[l].other, pl->lv[l - 1].other_tex, pl->lv[l].h, pl->lv[l].w, s),
-                 "downSamplingImage");
-
-  const int nIt = pl->prm.nSolverIters;
-  const int K = pl->variant;
-  const int npass = (nIt + K - 1) / K;
-  for (int l = L - 1; l >= 0; --l) {
-    auto& v = pl->lv[l];
-    const int h = v.h, w = v.w, b = l % 2;
-    const dim3 g = grid2d(h, w), blk(kBX, kBY);
-    if (l == L - 1) {  // warpUV, u, u_ <- 0 (Python/vfs.py:466-469)
-      VFS_TRY_CUDA(cudaMemset2DAsync(pl->ubefore[b].ptr, pl->ubefore[b].pitch, 0, (size_t)w * 4, h, s), "memset");
-      VFS_TRY_CUDA(cudaMemset2DAsync(pl->warp[b].ptr, pl->warp[b].pitch, 0, (size_t)w * 8, h, s), "memset");
-    }
-    Plane<const float> ub_src{pl->ubefore[b].ptr, pl->ubefore[b].pitch};
-    Plane<const uint8_t> mask{v.mask.ptr, v.mask.pitch};
-    // gaussian + computeTensorEtaMasked, Python/vfs.py:474-475
-    VFS_TRY_CUDA(launch_gaussian_masked(pl->smooth, v.ref_tex, mask, h, w, s), "gaussianMasked");
-    TgvConsts cst = pl->cst;
-    cst.code = v.code;
-    k_tensor_soa<<<g, blk, 0, s>>>(cst, v.code, v.smooth_tex, mask, kc, h, w);
-    VFS_TRY_CUDA(cudaGetLastError(), "tensor");
-    for (int wi = 0; wi < pl->prm.nWarpIters; ++wi) {
-      // findWarpingVector + warpingImage, Python/vfs.py:480-483
-      VFS_TRY_CUDA(launch_warp_prologue(Plane<float2>{pl->tvec.ptr, (size_t)w * 8}, pl->warped, {pl->warp[b].ptr, pl->warp[b].pitch}, v.tvf_tex, v.other_tex, h,
-                                        w, s),
-                   "warp prologue");
-      // computeDerivatives + solver reset, Python/vfs.py:486-497
-      k_derivs_init<<<g, blk, 0, s>>>(cst, pl->st[0], {pl->ubefore[b].ptr, pl->ubefore[b].pitch}, ub_src, v.ref_tex,
-                                      v.warped_tex, v.tvf_tex, h, w);
-      VFS_TRY_CUDA(cudaGetLastError(), "derivatives");
-      // solver iterations, Python/vfs.py:498-515
-      for (int j = 0; j < npass; ++j) {
-        const int it0 = j * K;
-        VFS_TRY_CUDA(launch_tgv_block(K, pl->st[j % 2], pl->st[(j + 1) % 2], cst, pl->sched, it0,
-                                      std::min(K, nIt - it0), kc, h, w, s),
-                     "tgv");
+  const size_t n0 = (size_t)v0.h * v0.w;
+  VFS_TRY_CUDA(cudaMemcpyAsync(pl->stage_ref, img_ref, n0, cudaMemcpyDeviceToDevice, s), "image copy");
+  VFS_TRY_CUDA(cudaMemcpyAsync(pl->stage_other, img_other, n0, cudaMemcpyDeviceToDevice, s), "image copy");
+  if (pl->use_graph) {
+    if (!pl->gstream) VFS_TRY_CUDA(cudaStreamCreateWithFlags(&pl->gstream, cudaStreamNonBlocking), "stream");
+    if (!pl->ev_in) VFS_TRY_CUDA(cudaEventCreateWithFlags(&pl->ev_in, cudaEventDisableTiming), "event");
+    if (!pl->ev_out) VFS_TRY_CUDA(cudaEventCreateWithFlags(&pl->ev_out, cudaEventDisableTiming), "event");
+    if (!pl->gexec) {
+      VFS_TRY_CUDA(cudaStreamBeginCapture(pl->gstream, cudaStreamCaptureModeThreadLocal), "begin capture");
+      int rc = enqueue_solve(pl, pl->gstream);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(pl->gstream, &g);
+      if (rc != VFS_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
       }
-      const TgvState& fin = pl->st[npass % 2];
-      // medianFilter + computeOpticalFlowWithClamp, Python/vfs.py:518-521
-      VFS_TRY_CUDA(launch_median_clamp({pl->warp[b].ptr, pl->warp[b].pitch}, pl->ubefore[b], {fin.u, (size_t)w * 4},
-                                       {pl->tvec.ptr, (size_t)w * 8}, mask, kc.upperLimit, h, w, s),
-                   "median/clamp");
-      ub_src = {fin.ub, (size_t)w * 4};
+      VFS_TRY_CUDA(e, "end capture");
+      e = cudaGraphInstantiate(&pl->gexec, g, 0);
+      cudaGraphDestroy(g);
+      VFS_TRY_CUDA(e, "graph instantiate");
     }
-    if (l > 0) {  // Python/vfs.py:523-528
-      auto& f = pl->lv[l - 1];
-      const int nb = (l - 1) % 2;
-      VFS_TRY_CUDA(launch_upsample1(pl->ubefore[nb], v.ubefore_tex, kc.fscale, f.h, f.w, s), "upSampling1");
-      VFS_TRY_CUDA(launch_upsample2(pl->warp[nb], v.warp_tex, kc.fscale, f.h, f.w, s), "upSampling");
-    }
+    VFS_TRY_CUDA(cudaEventRecord(pl->ev_in, s), "event record");
+    VFS_TRY_CUDA(cudaStreamWaitEvent(pl->gstream, pl->ev_in, 0), "stream wait");
+    VFS_TRY_CUDA(cudaGraphLaunch(pl->gexec, pl->gstream), "graph launch");
+    VFS_TRY_CUDA(cudaEventRecord(pl->ev_out, pl->gstream), "event record");
+    VFS_TRY_CUDA(cudaStreamWaitEvent(s, pl->ev_out, 0), "stream wait");
+  } else {
+    VFS_TRY(enqueue_solve(pl, s));
   }
-  // warpUV_ref[masks[0] == 0, :] = 0, Python/vfs.py:531
-  VFS_TRY_CUDA(launch_mask_flow(pl->warp[0], {v0.mask.ptr, v0.mask.pitch}, v0.h, v0.w, s), "mask flow");
   VFS_TRY_CUDA(cudaMemcpy2DAsync(warp_out, (size_t)v0.w * 8, pl->warp[0].ptr, pl->warp[0].pitch, (size_t)v0.w * 8,
                                  v0.h, cudaMemcpyDeviceToDevice, s),
                "flow copy");
   pl->solved = true;
+  return VFS_OK;
+}
+
+int vfs_plan_set_graph(VfsPlan* pl, int enable) {
+  if (!pl) return fail(VFS_ERR_ARG, "plan is NULL");
+  if ((bool)enable != pl->use_graph) pl->drop_graph();
+  pl->use_graph = enable != 0;
+  return VFS_OK;
+}
+
+int vfs_plan_set_timing(VfsPlan* pl, int enable) {
+  if (!pl) return fail(VFS_ERR_ARG, "plan is NULL");
+  if ((bool)enable != pl->timing) pl->drop_graph();
+  pl->timing = enable != 0;
+  if (pl->timing) {  // one event pair per warp, created before any capture
+    const size_t need = 2 * (size_t)pl->L * std::max(1, pl->prm.nWarpIters);
+    while (pl->tev.size() < need) {
+      cudaEvent_t e;
+      VFS_TRY_CUDA(cudaEventCreate(&e), "event create");
+      pl->tev.push_back(e);
+    }
+    pl->tev_bytes.resize(need / 2);
+    pl->tev_launches.resize(need / 2);
+  }
+  return VFS_OK;
+}
+
+int vfs_plan_stats(VfsPlan* pl, VfsSolveStats* out) {
+  if (!pl || !out) return fail(VFS_ERR_ARG, "NULL argument");
+  memset(out, 0, sizeof(*out));
+  out->kernels_per_solve = pl->kernels_per_solve;
+  if (!pl->timing) return VFS_OK;
+  double ms = 0, bytes = 0;
+  long long launches = 0;
+  for (int i = 0; i < pl->tev_used; ++i) {
+    float t = 0;
+    VFS_TRY_CUDA(cudaEventElapsedTime(&t, pl->tev[2 * i], pl->tev[2 * i + 1]), "event elapsed (synchronise first)");
+    ms += t;
+    bytes += pl->tev_bytes[i];
+    launches += pl->tev_launches[i];
+  }
+  out->tgv_ms = ms;
+  out->tgv_alg_bytes = bytes;
+  out->tgv_launches = launches;
+  out->tgv_intervals = pl->tev_used;
   return VFS_OK;
 }
 
@@ -381,3 +522,10 @@ int vfs_plan_triangulate(VfsPlan* pl, float f, float u0, float v0f, const float*
 }
 
 }  // extern "C"
+
+extern "C" int vfs_tgv_variants(int* ids, int cap, int* iters_per_launch) {
+  const int n = tgv_variant_list(ids, cap);
+  if (ids && iters_per_launch)
+    for (int i = 0; i < n && i < cap; ++i) iters_per_launch[i] = tgv_max_iters_per_launch(ids[i]);
+  return n;
+}

@@ -26,6 +26,8 @@
 //
 // Per-pixel arithmetic is vfs_pixel.cuh's, shared with the one-kernel-per-
 // step entry points, so the fused solver is bit-identical to them.
+#include <cstdio>
+
 #include "vfs_tgv.cuh"
 
 namespace vfs {
@@ -185,27 +187,92 @@ cudaError_t launch_block(const TgvState& in, const TgvState& out, const TgvConst
                          int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
   using G = TgvGeom<K, TX, TY>;
   const size_t smem = G::smem_bytes();
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_tgv_block<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
   dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);
   k_tgv_block<K, TX, TY, NT><<<grid, NT, smem, s>>>(in, out, c, sched, it0, niter, kc, h, w);
   return cudaGetLastError();
 }
 
 }  // namespace
+}  // namespace vfs
+
+#include "vfs_tgv_reg.cuh"
+
+namespace vfs {
+namespace {
+
+template <int K, int TX, int TY, int NT>
+cudaError_t prepare_block() {
+  return cudaFuncSetAttribute(k_tgv_block<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)TgvGeom<K, TX, TY>::smem_bytes());
+}
+
+template <int K, int TX, int TY, int NT>
+cudaError_t prepare_reg() {
+  return cudaFuncSetAttribute(k_tgv_reg<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)RegGeom<K, TX, TY>::smem_bytes());
+}
+
+template <int K, int TX, int TY, int NT>
+cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts& c, const float3* sched, int it0,
+                       int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
+  dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);
+  k_tgv_reg<K, TX, TY, NT><<<grid, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(in, out, c, sched, it0, niter, kc, h,
+                                                                               w);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, k_tgv_reg<K, TX, TY, NT>);
+    fprintf(stderr, "k_tgv_reg<%d,%d,%d,%d>: %s (smem %zu, max dyn %d, regs %d, max threads %d, local %zu)\n", K, TX,
+            TY, NT, cudaGetErrorString(e), RegGeom<K, TX, TY>::smem_bytes(), a.maxDynamicSharedSizeBytes, a.numRegs,
+            a.maxThreadsPerBlock, a.localSizeBytes);
+  }
+  return e;
+}
+
+// Compiled variants: id -> (implementation, iterations per launch, tile).
+// Ids below 100 keep all state in shared memory; ids 1xx are register-owned.
+#define VFS_TGV_VARIANTS(X)          \
+  X(1, block, 1, 32, 16, 256)        \
+  X(2, block, 2, 32, 32, 512)        \
+  X(4, block, 4, 32, 32, 512)        \
+  X(102, reg, 2, 32, 32, 512)        \
+  X(103, reg, 3, 32, 32, 512)        \
+  X(104, reg, 4, 32, 32, 512)        \
+  X(106, reg, 6, 32, 32, 512)        \
+  X(114, reg, 4, 64, 16, 512)        \
+  X(124, reg, 4, 32, 16, 256)        \
+  X(134, reg, 4, 32, 32, 1024)       \
+  X(122, reg, 2, 32, 16, 256)
+
+}  // namespace
+
+cudaError_t tgv_prepare() {
+  cudaError_t e = cudaSuccess;
+#define VFS_PREP(id, impl, K, TX, TY, NT) \
+  if (e == cudaSuccess) e = prepare_##impl<K, TX, TY, NT>();
+  VFS_TGV_VARIANTS(VFS_PREP)
+#undef VFS_PREP
+  return e;
+}
 
 int tgv_max_iters_per_launch(int variant) {
   switch (variant) {
-    case 1: return 1;
-    case 2: return 2;
-    case 4: return 4;
+#define VFS_ITERS(id, impl, K, TX, TY, NT) \
+  case id: return K;
+    VFS_TGV_VARIANTS(VFS_ITERS)
+#undef VFS_ITERS
     default: return 0;
   }
+}
+
+int tgv_variant_list(int* ids, int cap) {
+  int n = 0;
+#define VFS_LIST(id, impl, K, TX, TY, NT) \
+  if (ids && n < cap) ids[n] = id;       \
+  ++n;
+  VFS_TGV_VARIANTS(VFS_LIST)
+#undef VFS_LIST
+  return n;
 }
 
 cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& out, const TgvConsts& c,
@@ -213,9 +280,10 @@ cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& ou
                              cudaStream_t s) {
   if (h <= 0 || w <= 0 || niter <= 0) return cudaSuccess;
   switch (variant) {
-    case 1: return launch_block<1, 32, 16, 256>(in, out, c, sched, it0, niter, kc, h, w, s);
-    case 2: return launch_block<2, 32, 32, 512>(in, out, c, sched, it0, niter, kc, h, w, s);
-    case 4: return launch_block<4, 32, 32, 512>(in, out, c, sched, it0, niter, kc, h, w, s);
+#define VFS_LAUNCH_V(id, impl, K, TX, TY, NT) \
+  case id: return launch_##impl<K, TX, TY, NT>(in, out, c, sched, it0, niter, kc, h, w, s);
+    VFS_TGV_VARIANTS(VFS_LAUNCH_V)
+#undef VFS_LAUNCH_V
     default: return cudaErrorInvalidValue;
   }
 }

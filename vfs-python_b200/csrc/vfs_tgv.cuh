@@ -23,7 +23,12 @@ struct TgvConsts {
   const uint8_t* code;
 };
 
-// Iterations per launch of each compiled variant (0 if unknown).
+// Sets the kernels' shared-memory attributes (call before any graph capture).
+cudaError_t tgv_prepare();
+
+// Iterations per launch of each compiled variant (0 if unknown), and the
+// list of compiled variant ids (returns the count; writes up to cap ids).
+int tgv_variant_list(int* ids, int cap);
 int tgv_max_iters_per_launch(int variant);
 
 // Runs `niter` (<= the variant's K) iterations starting at schedule index

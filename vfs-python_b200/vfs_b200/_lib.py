@@ -41,6 +41,13 @@ class VfsParams(ctypes.Structure):
                    int(p.nWarpIters), int(p.nSolverIters))
 
 
+class VfsSolveStats(ctypes.Structure):
+    """Mirror of ``VfsSolveStats`` in include/vfs_b200.h."""
+    _fields_ = [("kernels_per_solve", ctypes.c_longlong), ("tgv_ms", ctypes.c_double),
+                ("tgv_alg_bytes", ctypes.c_double), ("tgv_launches", ctypes.c_longlong),
+                ("tgv_intervals", ctypes.c_int)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _F = ctypes.c_float
@@ -87,6 +94,10 @@ _SIGS = {
     "vfs_plan_solve": [_P, _P, _P, _P, _P],
     "vfs_plan_triangulate": [_P, _F, _F, _F, _P, _P, _P],
     "vfs_plan_set_tgv_variant": [_P, _I],
+    "vfs_plan_set_graph": [_P, _I],
+    "vfs_tgv_variants": [_P, _I, _P],
+    "vfs_plan_set_timing": [_P, _I],
+    "vfs_plan_stats": [_P, ctypes.POINTER(VfsSolveStats)],
     "vfs_step_schedule": [_I, _D, _P],
 }
 

@@ -41,6 +41,8 @@ class VFS:
         self._plan_mask = False
         self._plan_fields = False
         self.tgv_iters_per_launch = 4
+        self.use_graph = False
+        self.timing = False
 
     # ---- Python/vfs.py:38-74
     def setup_module(self):
@@ -92,9 +94,32 @@ class VFS:
         call("vfs_plan_create", ctypes.byref(prm), self._workspace.data_ptr(), self._workspace.numel(),
              ctypes.byref(plan))
         call("vfs_plan_set_tgv_variant", plan, int(self.tgv_iters_per_launch))
+        call("vfs_plan_set_graph", plan, 1 if self.use_graph else 0)
+        call("vfs_plan_set_timing", plan, 1 if self.timing else 0)
         self._plan, self._plan_key = plan, key
         self._plan_mask = self._plan_fields = False
         return plan
+
+    def configure(self, iters_per_launch=None, use_graph=None, timing=None):
+        """Fused-path options: TGV iterations per launch (1, 2, 4), CUDA-graph
+        replay of the whole solve, and TGV event timing (see ``solve_stats``)."""
+        if iters_per_launch is not None:
+            self.tgv_iters_per_launch = int(iters_per_launch)
+        if use_graph is not None:
+            self.use_graph = bool(use_graph)
+        if timing is not None:
+            self.timing = bool(timing)
+        if self._plan is not None:
+            call("vfs_plan_set_tgv_variant", self._plan, int(self.tgv_iters_per_launch))
+            call("vfs_plan_set_graph", self._plan, 1 if self.use_graph else 0)
+            call("vfs_plan_set_timing", self._plan, 1 if self.timing else 0)
+
+    def solve_stats(self) -> dict:
+        """Statistics of the last fused solve (synchronises the current stream)."""
+        torch.cuda.current_stream().synchronize()
+        st = _lib.VfsSolveStats()
+        call("vfs_plan_stats", self._plan, ctypes.byref(st))
+        return {k: getattr(st, k) for k, _ in st._fields_}
 
     def release(self):
         """Frees the plan (and its workspace)."""
