@@ -176,6 +176,23 @@ typedef struct VfsSolveStats {
 } VfsSolveStats;
 /* Statistics of the last solve; synchronise its stream first. */
 VFS_API int vfs_plan_stats(VfsPlan* plan, VfsSolveStats* out);
+/* ---- whole solve with no device allocation --------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a real-time loop with a fixed memory budget, a host callback, a foreign
+ * runtime that owns no CUDA allocator): the same solve as vfs_plan_create +
+ * vfs_plan_set_mask + vfs_plan_set_vector_fields + vfs_plan_solve, with the
+ * workspace taken from a scratch array of vfs_static_scratch_bytes() (32 MiB)
+ * compiled into the library and held by every GPU that loads it until the
+ * process exits.  Sizes whose workspace does not fit (see
+ * vfs_plan_workspace_size) are rejected with VFS_ERR_WORKSPACE.  The first call
+ * on a device (and the first after a parameter change) sets up a plan over the
+ * scratch and uploads the step sizes with a synchronous copy, so make it
+ * before any stream capture.  All calls on a device share the scratch: calls
+ * whose GPU work overlaps race, so issue them on one stream or order them. */
+VFS_API size_t vfs_static_scratch_bytes(void);
+VFS_API int vfs_solve_stereo_static(const VfsParams* prm, const uint8_t* mask, size_t mask_pitch,
+                                    const float* tvf_hw2, const float* cvf_hw2, const uint8_t* img_ref,
+                                    const uint8_t* img_other, float* warp_out_hw2, void* stream);
 /* Compiled fused-TGV kernel variants: returns their number and writes up to
  * `cap` ids and their iterations per launch. */
 VFS_API int vfs_tgv_variants(int* ids, int cap, int* iters_per_launch);

@@ -96,6 +96,8 @@ _SIGS = {
     "vfs_plan_set_tgv_variant": [_P, _I],
     "vfs_plan_set_graph": [_P, _I],
     "vfs_tgv_variants": [_P, _I, _P],
+    "vfs_static_scratch_bytes": [],
+    "vfs_solve_stereo_static": [_PRM, _P, _SZ, _P, _P, _P, _P, _P, _P],
     "vfs_plan_set_timing": [_P, _I],
     "vfs_plan_stats": [_P, ctypes.POINTER(VfsSolveStats)],
     "vfs_step_schedule": [_I, _D, _P],
@@ -115,7 +117,8 @@ def lib() -> ctypes.CDLL:
         for name, args in _SIGS.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = ctypes.c_char_p if name == "vfs_last_error" else ctypes.c_int
+            fn.restype = (ctypes.c_char_p if name == "vfs_last_error" else
+                          ctypes.c_size_t if name == "vfs_static_scratch_bytes" else ctypes.c_int)
         _lib = L
     return _lib
 
