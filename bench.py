@@ -236,7 +236,7 @@ def cpu_baseline_sample(pair, p, budget_s=20.0):
 
 
 def load_traffic():
-    path = os.path.join(ROOT, "profiles", "k_tgv_block_800x800_ncu.json")
+    path = os.path.join(ROOT, "profiles", "k_tgv_reg_800x800_ncu.json")
     try:
         with open(path) as f:
             return json.load(f)
@@ -403,7 +403,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--iters-per-launch", type=int, default=4)
+    ap.add_argument("--iters-per-launch", type=int, default=134)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)

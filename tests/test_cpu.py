@@ -1,0 +1,208 @@
+"""CPU tests: the C ABI's host side, the step schedule, and the float64 oracle
+pinned against golden outputs of the reference's own kernels.
+
+No GPU is used.  tests/golden/ref_small.npz was produced on a B200 by
+tests/golden/make_golden.py from the reference's CUDA kernels (built from its
+sources) with the reference's host call order.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import bench_params, default_params, pair
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "vfs_b200.h")
+GOLDEN = os.path.join(ROOT, "tests", "golden", "ref_small.npz")
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from vfs_b200 import _lib
+    return _lib
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return dict(np.load(GOLDEN))
+
+
+# ---------------------------------------------------------------- C ABI, host side
+def test_library_exports_every_header_symbol(lib):
+    declared = re.findall(r"VFS_API\s+(?:int|size_t|const char\*)\s+(vfs_\w+)", open(HEADER).read())
+    assert len(declared) >= 40
+    out = subprocess.run(["nm", "-D", "--defined-only", lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert sorted(set(declared) - exported) == []
+    assert sorted(exported - set(declared)) == []
+    L = lib.lib()
+    for name in declared:
+        assert hasattr(L, name)
+
+
+def test_step_schedule_matches_reference_numpy_rules(lib):
+    from oracle.np64.vfs64 import step_schedule
+    for n, tsl in [(100, 1.0), (50, 1.0), (7, 0.3), (3000, 3.0)]:
+        out = np.zeros(3 * n, np.float32)
+        lib.call("vfs_step_schedule", n, tsl, out.ctypes.data)
+        want = np.array(step_schedule(n, tsl), np.float32).reshape(-1)
+        assert np.array_equal(out.view(np.uint32), want.view(np.uint32))
+
+
+def _prm(lib, **kw):
+    p = bench_params(64, 80, n_level=3)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return lib.VfsParams.from_param_bag(p)
+
+
+def test_workspace_size_and_parameter_validation(lib):
+    n = ctypes.c_size_t(0)
+    lib.call("vfs_plan_workspace_size", ctypes.byref(_prm(lib)), ctypes.byref(n))
+    small = n.value
+    lib.call("vfs_plan_workspace_size", ctypes.byref(_prm(lib, width=800, height=800)), ctypes.byref(n))
+    assert n.value > 50 * small
+    for bad in (dict(width=0), dict(nLevel=0), dict(fScale=1.0), dict(nSolverIters=-1), dict(Lambda=float("nan")),
+                dict(nLevel=12)):  # 64 / 2**11 == 0: a level of size zero
+        with pytest.raises(ValueError):
+            lib.call("vfs_plan_workspace_size", ctypes.byref(_prm(lib, **bad)), ctypes.byref(n))
+
+
+def test_plan_create_rejects_missing_workspace(lib):
+    plan = ctypes.c_void_p(0)
+    rc = lib.lib().vfs_plan_create(ctypes.byref(_prm(lib)), None, 0, ctypes.byref(plan))
+    assert rc == lib.VFS_ERR_WORKSPACE
+    assert "workspace of" in lib.lib().vfs_last_error().decode()
+
+
+def test_static_solve_rejects_oversize_before_touching_cuda(lib):
+    p = lib.VfsParams.from_param_bag(bench_params(2048, 2048, n_level=5, n_warp=1, n_iter=1))
+    dummy = ctypes.c_void_p(16)
+    rc = lib.lib().vfs_solve_stereo_static(ctypes.byref(p), dummy, 2048, dummy, dummy, dummy, dummy, dummy, None)
+    assert rc == lib.VFS_ERR_WORKSPACE
+
+
+def test_null_arguments_are_rejected(lib):
+    rc = lib.lib().vfs_cast_and_scale(None, None, 4, 4, None)
+    assert rc == lib.VFS_ERR_ARG
+    # texture bases must be 512-byte aligned and pitches multiples of 32 bytes
+    # covering a row; both are checked before any CUDA call
+    tex = ctypes.c_uint64()
+    rc = lib.lib().vfs_texture_create(ctypes.c_void_p(0x1100), 4, 4, 64, 2, 1, ctypes.byref(tex))
+    assert rc == lib.VFS_ERR_ALIGN
+    rc = lib.lib().vfs_texture_create(ctypes.c_void_p(0x1000), 4, 8, 20, 2, 1, ctypes.byref(tex))
+    assert rc == lib.VFS_ERR_ALIGN
+    rc = lib.lib().vfs_texture_create(ctypes.c_void_p(0x1000), 4, 8, 32, 7, 1, ctypes.byref(tex))
+    assert rc == lib.VFS_ERR_ARG
+
+
+def test_synthetic_pairs_are_deterministic():
+    a = pair(64, seed=3)
+    b = pair(64, seed=3)
+    c = pair(64, seed=4)
+    assert np.array_equal(a.img_ref, b.img_ref) and np.array_equal(a.img_other, b.img_other)
+    assert not np.array_equal(a.img_ref, c.img_ref)
+    assert a.img_ref.dtype == np.uint8 and a.mask.max() == 255
+
+
+# ---------------------------------------------------------------- oracle vs golden
+def _within(a, b, atol, frac=1.0, what=""):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    assert a.shape == b.shape, what
+    ok = np.abs(a - b) <= atol
+    assert ok.mean() >= frac, f"{what}: {100 * (1 - ok.mean()):.3f}% beyond {atol}, max {np.abs(a - b).max()}"
+
+
+def test_oracle_mask_pyramid_exact(gold):
+    from oracle.np64 import vfs64 as V
+    m = gold["mask_0"]
+    for k in (1, 2):
+        h, w = gold[f"mask_{k}"].shape
+        got = V.down_sampling_mask(gold[f"mask_{k - 1}"], h, w)
+        assert np.array_equal(got, gold[f"mask_{k}"]), f"mask level {k}"
+    assert np.array_equal(m, gold["mask"])
+
+
+def test_oracle_pyramids(gold):
+    from oracle.np64 import vfs64 as V
+    for k in (1, 2):
+        h, w = gold[f"ref_{k}"].shape
+        _within(V.down_sampling(gold[f"ref_{k - 1}"], h, w, "tex8"), gold[f"ref_{k}"], 2e-3, what=f"ref {k}")
+        _within(V.down_sampling(gold[f"other_{k - 1}"], h, w, "tex8"), gold[f"other_{k}"], 2e-3, what=f"other {k}")
+        _within(V.down_sampling(gold[f"tvf_{k - 1}"], h, w, "tex8"), gold[f"tvf_{k}"], 2e-3, what=f"tvf {k}")
+    _within(V.cast_and_scale(gold["img_ref"]), gold["ref_0"], 0, what="castAndScale")
+    _within(V.warping_image(V.cast_and_scale(gold["img_other"]), gold["cvf"], "tex8"), gold["other_0"], 2e-3,
+            what="calibration warp")
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_oracle_step_kernels(gold, k):
+    from oracle.np64 import vfs64 as V
+    prm = bench_params(*gold[f"ref_{k}"].shape, n_level=3)
+    M = gold[f"mask_{k}"]
+    g = lambda n: gold[f"L{k}_out_{n}"]
+    i = lambda n: gold[f"L{k}_in_{n}"].astype(np.float64)
+    _within(V.gaussian_masked(gold[f"ref_{k}"], M, "tex8"), g("smooth"), 1e-6, what="gaussian")
+    abc, eta = V.compute_tensor_eta(g("smooth"), M, prm, "tex8")
+    _within(abc, g("abc"), 2e-5, what="tensor")
+    _within(eta, g("eta"), 2e-5 * np.abs(g("eta")).max(), what="eta")
+    _within(V.find_warping_vector(gold[f"tvf_{k}"], i("warp"), "tex8"), g("tvec"), 2e-3, what="findWarpingVector")
+    _within(V.warping_image(gold[f"other_{k}"], i("warp"), "tex8"), g("warped"), 3e-3, what="warpingImage")
+    d = V.compute_derivatives(gold[f"ref_{k}"], g("warped"), gold[f"tvf_{k}"], "tex8")
+    _within(d, g("deriv"), 3e-3, frac=0.999, what="computeDerivatives")
+    sigma, tau, mu = (float(v) for v in gold[f"L{k}_sched"])
+    # the solver steps have no texture reads: float64 vs float32 on identical inputs
+    p, tp, q = V.update_dual_variables(i("p"), i("q"), sigma, i("ub"), i("vb"), g("abc"), M, prm)
+    _within(p, g("p"), 1e-5, what="dual p")
+    _within(tp, g("tp"), 1e-5, what="dual tp")
+    _within(q, g("q"), 1e-5, what="dual q")
+    u = V.l1_thresholding(tau, g("tp"), i("u"), i("ub"), g("deriv"), g("eta"), M, prm)
+    _within(u, g("u"), 1e-4, frac=0.999, what="threshold")
+    ub, vb = V.update_primal_variables(tau, mu, g("p"), g("q"), g("u"), i("ub"), i("vb"), g("abc"), g("eta"), M, prm)
+    _within(ub, g("ub"), 1e-4, what="primal u_")
+    _within(vb, g("vb"), 1e-4, what="primal v_")
+    med = V.median_filter(g("u").astype(np.float64), M)
+    assert np.array_equal(med.astype(np.float32), g("median"))
+    warp = i("warp").copy()
+    ubf = i("ub").copy()
+    V.compute_optical_flow_with_clamp(warp, ubf, g("median").astype(np.float64), g("tvec").astype(np.float64), M,
+                                      prm)
+    _within(warp, g("clamp_warp"), 1e-5, what="clamp warp")
+    _within(ubf, g("clamp_u"), 1e-5, what="clamp u")
+    if k > 0:
+        fh, fw = gold[f"ref_{k - 1}"].shape
+        _within(V.upsampling(g("clamp_u"), fh, fw, 2.0, "tex8"), g("up1"), 1e-5, what="upsample1")
+        _within(V.upsampling(g("clamp_warp"), fh, fw, 2.0, "tex8"), g("up2"), 1e-5, what="upsample2")
+
+
+def test_oracle_camera(gold):
+    from oracle.np64 import vfs64 as V
+    cam = V.EquidistantCam64(gold["intrinsics"])
+    h, w = gold["mask"].shape
+    _within(cam.get_rays((h, w)), gold["cam_rays"], 2e-6, what="rays")
+    xyz = cam.unproject(gold["cam_uv_in"].astype(np.float64))
+    _within(xyz, gold["cam_xyz"], 2e-6, what="getXYZFromUV")
+    _within(cam.project(gold["cam_xyz"].astype(np.float64)), gold["cam_uv"], 2e-4, what="getUVFromXYZ")
+
+
+def test_oracle_end_to_end_default_params(gold):
+    """The whole reference-default solve (Lambda 5, fScale 1.2) in float64 stays
+    close to the reference kernels' float32 result."""
+    from oracle.np64 import vfs64 as V
+    h, w = gold["mask"].shape
+    prm = default_params(h, w, n_level=4, n_warp=2, n_iter=9)
+    v = V.VFS64(prm, "tex8")
+    v.compute_pyramid_sizes()
+    v.create_mask_pyramid(gold["mask"])
+    v.create_vector_field_pyramid(gold["tvf"], gold["cvf"])
+    warp = v.solve_stereo(gold["img_ref"], gold["img_other"])
+    m = gold["mask"] > 0
+    d = np.abs(warp - gold["e2e_default_warp"])[m]
+    assert np.median(d) < 1e-3 and np.percentile(d, 99) < 0.05, (np.median(d), np.percentile(d, 99))
