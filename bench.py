@@ -251,6 +251,7 @@ def run_b200(args, n, rank, local):
     vfs.configure(iters_per_launch=args.iters_per_launch, use_graph=not args.no_graph, timing=True)
     ref_d = torch.as_tensor(pair.img_ref).cuda()
     oth_d = torch.as_tensor(pair.img_other).cuda()
+    level_choice = vfs.autotune(ref_d, oth_d) if not args.no_autotune else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
@@ -325,7 +326,8 @@ def run_b200(args, n, rank, local):
         "config": {"workload": "800x800 equidistant fisheye pair, 5 levels x 10 warps x 100 TGV iterations, "
                                "solve_stereo + triangulate_flow",
                    "size": SIZE, "levels": N_LEVEL, "warps": N_WARP, "iterations": N_ITER, "lambda": 50.0,
-                   "t": list(T), "tgv_iters_per_launch": args.iters_per_launch, "cuda_graph": not args.no_graph,
+                   "t": list(T), "tgv_kernel_default": args.iters_per_launch,
+                   "tgv_kernel_per_level": level_choice, "cuda_graph": not args.no_graph,
                    "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "parallelism": f"dp{n} (independent pairs)"},
         "roofline": {"bound": "hbm", "kernel": "k_tgv_block (fused TGV iterations)",
@@ -405,6 +407,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--iters-per-launch", type=int, default=134)
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     args = ap.parse_args()

@@ -173,6 +173,7 @@ typedef struct VfsSolveStats {
   double tgv_alg_bytes;        /* their algorithmic bytes: 113 per pixel-iteration */
   long long tgv_launches;      /* number of TGV kernel launches timed */
   int tgv_intervals;           /* event pairs summed */
+  double tgv_ms_level[16];     /* tgv_ms split by pyramid level (0 = finest) */
 } VfsSolveStats;
 /* Statistics of the last solve; synchronise its stream first. */
 VFS_API int vfs_plan_stats(VfsPlan* plan, VfsSolveStats* out);
@@ -196,6 +197,17 @@ VFS_API int vfs_solve_stereo_static(const VfsParams* prm, const uint8_t* mask, s
 /* Compiled fused-TGV kernel variants: returns their number and writes up to
  * `cap` ids and their iterations per launch. */
 VFS_API int vfs_tgv_variants(int* ids, int cap, int* iters_per_launch);
+/* Run levels that fit in one thread-block cluster with the cluster-resident
+ * kernel (all iterations, median and clamp in one launch) unless a per-level
+ * variant is set; off by default. */
+VFS_API int vfs_plan_set_cluster(VfsPlan* plan, int enable);
+/* Per-level TGV kernel: a variant id, VFS_TGV_CLUSTER for the cluster-resident
+ * kernel (used where the level fits in one cluster), or 0 for the plan's
+ * variant.  Level 0 is the finest. */
+#define VFS_TGV_CLUSTER 1000
+VFS_API int vfs_plan_set_level_variant(VfsPlan* plan, int level, int variant);
+/* Cluster size the cluster-resident kernel would use for a level (0: does not fit). */
+VFS_API int vfs_plan_level_cluster(const VfsPlan* plan, int level);
 /* Select the fused TGV kernel variant by id (see vfs_tgv_variants). */
 VFS_API int vfs_plan_set_tgv_variant(VfsPlan* plan, int iters_per_launch);
 

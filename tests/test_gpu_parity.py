@@ -165,7 +165,8 @@ def test_step_kernels_bit_exact(ref_mod, all_ones_mask):
                               f"upsample2 L{k}")
 
 
-def _solve_pair(ref_mod, prm, p, lib_name=None, mask=None, variants=(4,)):
+def _solve_pair(ref_mod, prm, p, lib_name=None, mask=None, variants=((4, False),)):
+    """Reference solve vs the fused solve under each (TGV variant, cluster) config."""
     from vfs_b200.equidistant_cam import EquidistantCam
     r, o = _both(ref_mod, prm, p, lib_name=lib_name, mask=mask)
     rw = _np(r.solve_stereo(p.img_ref, p.img_other))
@@ -175,15 +176,16 @@ def _solve_pair(ref_mod, prm, p, lib_name=None, mask=None, variants=(4,)):
     cam = EquidistantCam(p.intrinsics)
     cam.setup_module()
     outs = {}
-    for v in variants:
+    for v, cluster in variants:
         o.tgv_iters_per_launch = v
+        o.use_cluster = cluster
         o.release()
         try:
             ow = _np(o.solve_stereo(p.img_ref, p.img_other))
         except Exception as e:
-            raise AssertionError(f"TGV variant {v}: {e}") from e
+            raise AssertionError(f"TGV variant {v} (cluster {cluster}): {e}") from e
         oxyz = _np(o.triangulate_flow(cam, p.t))
-        outs[v] = (ow, oxyz)
+        outs[(v, cluster)] = (ow, oxyz)
     return (rw, rxyz), outs, o, cam
 
 
@@ -196,7 +198,8 @@ def test_solve_bit_exact_bench_params(ref_mod, n_iter):
     import ctypes
     ids = (ctypes.c_int * 64)()
     n = _lib.lib().vfs_tgv_variants(ids, 64, None)
-    (rw, rxyz), outs, o, cam = _solve_pair(ref_mod, prm, p, variants=tuple(ids[i] for i in range(n)))
+    configs = [(ids[i], False) for i in range(n)] + [(134, True)]
+    (rw, rxyz), outs, o, cam = _solve_pair(ref_mod, prm, p, variants=configs)
     for v, (ow, oxyz) in outs.items():
         assert_bits_equal(rw, ow, f"warpUV (iterations per launch {v})")
         assert_bits_equal(rxyz, oxyz, f"xyz (iterations per launch {v})")
@@ -211,10 +214,11 @@ def test_solve_bit_exact_default_params(ref_mod):
     h, w = 90, 100
     p = pair(w, height=h, seed=2, n_level=6)
     prm = default_params(h, w, n_level=6, n_warp=2, n_iter=9)
-    (rw, rxyz), outs, _, _ = _solve_pair(ref_mod, prm, p, lib_name="default")
-    ow, oxyz = outs[4]
-    assert_bits_equal(rw, ow, "warpUV")
-    assert_bits_equal(rxyz, oxyz, "xyz")
+    (rw, rxyz), outs, _, _ = _solve_pair(ref_mod, prm, p, lib_name="default",
+                                         variants=((4, False), (134, False), (134, True)))
+    for v, (ow, oxyz) in outs.items():
+        assert_bits_equal(rw, ow, f"warpUV {v}")
+        assert_bits_equal(rxyz, oxyz, f"xyz {v}")
 
 
 def test_solve_bit_exact_all_ones_mask(ref_mod):
@@ -223,7 +227,7 @@ def test_solve_bit_exact_all_ones_mask(ref_mod):
     p = pair(w, height=h, seed=4, n_level=3)
     prm = bench_params(h, w, n_level=3, n_warp=2, n_iter=10)
     ones = np.full((h, w), 255, np.uint8)
-    (rw, rxyz), outs, _, _ = _solve_pair(ref_mod, prm, p, mask=ones, variants=(1, 4))
+    (rw, rxyz), outs, _, _ = _solve_pair(ref_mod, prm, p, mask=ones, variants=((1, False), (4, False), (134, True)))
     for v, (ow, oxyz) in outs.items():
         assert_bits_equal(rw, ow, f"warpUV (iterations per launch {v})")
         assert_bits_equal(rxyz, oxyz, f"xyz (iterations per launch {v})")
@@ -263,3 +267,23 @@ def test_camera_and_vector_fields(ref_mod):
         ot, ocv = get_vector_fields(gridf((h, w)), oc, oc, Rm, np.asarray(t), ts)
         assert np.nanmax(np.abs(rt - ot)) < 5e-4
         assert np.nanmax(np.abs(rcv - ocv)) < 5e-4
+
+
+def test_autotuned_levels_bit_exact(ref_mod):
+    """The autotuner's per-level kernel choice (tiles, iterations per launch,
+    cluster kernel) changes speed only: the solve stays bit-identical."""
+    from vfs_b200.autotune import variants, CLUSTER
+    h, w = 96, 128
+    p = pair(w, height=h, t=(0.12, 0.01, 0.0), seed=6, n_level=3)
+    prm = bench_params(h, w, n_level=3, n_warp=2, n_iter=11)
+    r, o = _both(ref_mod, prm, p)
+    rw = _np(r.solve_stereo(p.img_ref, p.img_other))
+    choice = o.autotune(p.img_ref, p.img_other, repeats=1)
+    assert len(choice) == prm.nLevel
+    assert all(c in variants() or c == CLUSTER for c in choice)
+    o.configure(use_graph=True)
+    assert_bits_equal(rw, _np(o.solve_stereo(p.img_ref, p.img_other)), f"warpUV with {choice}")
+    # every single choice applied to all levels agrees as well
+    for c in (162, 192, CLUSTER):
+        o.set_level_variants([c] * prm.nLevel)
+        assert_bits_equal(rw, _np(o.solve_stereo(p.img_ref, p.img_other)), f"warpUV with {c} everywhere")

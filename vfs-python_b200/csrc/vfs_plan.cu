@@ -108,7 +108,8 @@ struct VfsPlan {
   Plane<float> ubefore[2];
   Plane<float2> warp[2];
   float3* sched = nullptr;
-  int variant = 4;
+  int variant = 134;
+  int level_variant[32] = {0};  // 0: the plan's variant; VFS_TGV_CLUSTER: cluster kernel
   bool mask_set = false, fields_set = false, solved = false;
   std::vector<cudaTextureObject_t> textures;
   // input staging (workspace), so a captured graph has fixed pointers
@@ -125,7 +126,11 @@ struct VfsPlan {
   std::vector<double> tev_bytes;
   std::vector<long long> tev_launches;
   int tev_used = 0;
+  std::vector<int> tev_level;
   long long kernels_per_solve = 0;
+  // cluster-resident solve for levels that fit one cluster
+  bool use_cluster = false;
+  int max_cluster = 0;
 
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -214,12 +219,20 @@ int enqueue_solve(VfsPlan* pl, cudaStream_t s) {
                  "downSamplingImage");
 
   const int nIt = pl->prm.nSolverIters;
-  const int K = tgv_max_iters_per_launch(pl->variant);
-  const int npass = (nIt + K - 1) / K;
   for (int l = L - 1; l >= 0; --l) {
     auto& v = pl->lv[l];
     const int h = v.h, w = v.w, b = l % 2;
     const dim3 g = grid2d(h, w), blk(kBX, kBY);
+    // TGV kernel for this level: the plan's variant, a per-level choice (the
+    // autotuner's), or the cluster-resident kernel where the level fits
+    int var = pl->level_variant[l] ? pl->level_variant[l] : pl->variant;
+    int cs = 0;
+    if (var == VFS_TGV_CLUSTER || (pl->level_variant[l] == 0 && pl->use_cluster)) {
+      cs = tgv_cluster_size(h, w, pl->max_cluster);
+      if (var == VFS_TGV_CLUSTER) var = pl->variant;
+    }
+    const int K = tgv_max_iters_per_launch(var);
+    const int npass = (nIt + K - 1) / K;
     if (l == L - 1) {  // warpUV, u, u_ <- 0 (Python/vfs.py:466-469)
       VFS_TRY_CUDA(cudaMemset2DAsync(pl->ubefore[b].ptr, pl->ubefore[b].pitch, 0, (size_t)w * 4, h, s), "memset");
       VFS_TRY_CUDA(cudaMemset2DAsync(pl->warp[b].ptr, pl->warp[b].pitch, 0, (size_t)w * 8, h, s), "memset");
@@ -244,7 +257,8 @@ int enqueue_solve(VfsPlan* pl, cudaStream_t s) {
       VFS_TRY_CUDA(cudaGetLastError(), "derivatives");
       nk += 2;
       // solver iterations, Python/vfs.py:498-515
-      const bool timed = pl->timing && npass > 0;
+      const int launches = cs > 0 ? 1 : npass;
+      const bool timed = pl->timing && launches > 0;
       if (timed) {
         const int pair = pl->tev_used;
         while ((int)pl->tev.size() < 2 * (pair + 1)) {
@@ -255,31 +269,46 @@ int enqueue_solve(VfsPlan* pl, cudaStream_t s) {
         if ((int)pl->tev_bytes.size() < pair + 1) {
           pl->tev_bytes.resize(pair + 1);
           pl->tev_launches.resize(pair + 1);
+          pl->tev_level.resize(pair + 1);
         }
         VFS_TRY_CUDA(cudaEventRecordWithFlags(pl->tev[2 * pair], s, cudaEventRecordExternal), "event record");
       }
-      for (int j = 0; j < npass; ++j) {
-        const int it0 = j * K;
-        VFS_TRY_CUDA(launch_tgv_block(pl->variant, pl->st[j % 2], pl->st[(j + 1) % 2], cst, pl->sched, it0,
-                                      std::min(K, nIt - it0), kc, h, w, s),
-                     "tgv");
+      if (cs > 0) {
+        // the whole level in one cluster: iterations + median + clamp
+        VFS_TRY_CUDA(launch_tgv_cluster(cs, pl->st[0], cst, pl->sched, nIt, kc, {pl->warp[b].ptr, pl->warp[b].pitch},
+                                        pl->ubefore[b], {pl->tvec.ptr, (size_t)w * 8}, kc.upperLimit, h, w, s),
+                     "tgv cluster");
+        ++nk;
+      } else {
+        for (int j = 0; j < npass; ++j) {
+          const int it0 = j * K;
+          VFS_TRY_CUDA(launch_tgv_block(var, pl->st[j % 2], pl->st[(j + 1) % 2], cst, pl->sched, it0,
+                                        std::min(K, nIt - it0), kc, h, w, s),
+                       "tgv");
+        }
+        nk += npass;
       }
-      nk += npass;
       if (timed) {
         const int pair = pl->tev_used++;
         VFS_TRY_CUDA(cudaEventRecordWithFlags(pl->tev[2 * pair + 1], s, cudaEventRecordExternal), "event record");
         // algorithmic bytes: 113 per pixel per iteration (state in and out,
         // per-warp constants in)
         pl->tev_bytes[pair] = 113.0 * (double)h * w * nIt;
-        pl->tev_launches[pair] = npass;
+        pl->tev_launches[pair] = launches;
+        pl->tev_level[pair] = l;
       }
-      const TgvState& fin = pl->st[npass % 2];
-      // medianFilter + computeOpticalFlowWithClamp, Python/vfs.py:518-521
-      VFS_TRY_CUDA(launch_median_clamp({pl->warp[b].ptr, pl->warp[b].pitch}, pl->ubefore[b], {fin.u, (size_t)w * 4},
-                                       {pl->tvec.ptr, (size_t)w * 8}, mask, kc.upperLimit, h, w, s),
-                   "median/clamp");
-      ++nk;
-      ub_src = {fin.ub, (size_t)w * 4};
+      if (cs > 0) {
+        ub_src = {pl->st[0].ub, (size_t)w * 4};
+      } else {
+        const TgvState& fin = pl->st[npass % 2];
+        // medianFilter + computeOpticalFlowWithClamp, Python/vfs.py:518-521
+        VFS_TRY_CUDA(launch_median_clamp({pl->warp[b].ptr, pl->warp[b].pitch}, pl->ubefore[b],
+                                         {fin.u, (size_t)w * 4}, {pl->tvec.ptr, (size_t)w * 8}, mask, kc.upperLimit,
+                                         h, w, s),
+                     "median/clamp");
+        ++nk;
+        ub_src = {fin.ub, (size_t)w * 4};
+      }
     }
     if (l > 0) {  // Python/vfs.py:523-528
       auto& f = pl->lv[l - 1];
@@ -351,6 +380,7 @@ int vfs_plan_create(const VfsParams* prm, void* workspace, size_t workspace_byte
       rc = make_tex(pl, pl->warp[l % 2].ptr, v.h, v.w, pl->warp[l % 2].pitch, VFS_TEX_F32X2, 1, &v.warp_tex);
   }
   if (rc == VFS_OK) rc = cuda_status(tgv_prepare(), "tgv kernel attributes");
+  if (rc == VFS_OK) rc = cuda_status(tgv_cluster_prepare(&pl->max_cluster), "cluster kernel attributes");
   if (rc == VFS_OK)
     rc = make_tex(pl, pl->other0.ptr, pl->lv[0].h, pl->lv[0].w, pl->other0.pitch, VFS_TEX_F32, 1, &pl->other0_tex);
   if (rc != VFS_OK) {
@@ -385,6 +415,7 @@ int vfs_plan_sizes(const VfsPlan* pl, int* hw) {
 int vfs_plan_set_tgv_variant(VfsPlan* pl, int k) {
   if (!pl) return fail(VFS_ERR_ARG, "plan is NULL");
   if (tgv_max_iters_per_launch(k) == 0) return fail(VFS_ERR_ARG, "unknown TGV kernel variant");
+  if (pl->variant != k) pl->drop_graph();
   pl->variant = k;
   return VFS_OK;
 }
@@ -484,6 +515,7 @@ int vfs_plan_set_timing(VfsPlan* pl, int enable) {
       pl->tev.push_back(e);
     }
     pl->tev_bytes.resize(need / 2);
+    pl->tev_level.resize(need / 2);
     pl->tev_launches.resize(need / 2);
   }
   return VFS_OK;
@@ -502,6 +534,8 @@ int vfs_plan_stats(VfsPlan* pl, VfsSolveStats* out) {
     ms += t;
     bytes += pl->tev_bytes[i];
     launches += pl->tev_launches[i];
+    const int lvl = pl->tev_level[i];
+    if (lvl >= 0 && lvl < 16) out->tgv_ms_level[lvl] += t;
   }
   out->tgv_ms = ms;
   out->tgv_alg_bytes = bytes;
@@ -528,4 +562,26 @@ extern "C" int vfs_tgv_variants(int* ids, int cap, int* iters_per_launch) {
   if (ids && iters_per_launch)
     for (int i = 0; i < n && i < cap; ++i) iters_per_launch[i] = tgv_max_iters_per_launch(ids[i]);
   return n;
+}
+
+extern "C" int vfs_plan_set_cluster(VfsPlan* pl, int enable) {
+  if (!pl) return fail(VFS_ERR_ARG, "plan is NULL");
+  if ((bool)enable != pl->use_cluster) pl->drop_graph();
+  pl->use_cluster = enable != 0;
+  return VFS_OK;
+}
+
+extern "C" int vfs_plan_set_level_variant(VfsPlan* pl, int level, int variant) {
+  if (!pl) return fail(VFS_ERR_ARG, "plan is NULL");
+  if (level < 0 || level >= pl->L) return fail(VFS_ERR_ARG, "level out of range");
+  if (variant != 0 && variant != VFS_TGV_CLUSTER && tgv_max_iters_per_launch(variant) == 0)
+    return fail(VFS_ERR_ARG, "unknown TGV kernel variant");
+  if (pl->level_variant[level] != variant) pl->drop_graph();
+  pl->level_variant[level] = variant;
+  return VFS_OK;
+}
+
+extern "C" int vfs_plan_level_cluster(const VfsPlan* pl, int level) {
+  if (!pl || level < 0 || level >= pl->L) return 0;
+  return tgv_cluster_size(pl->lv[level].h, pl->lv[level].w, pl->max_cluster);
 }

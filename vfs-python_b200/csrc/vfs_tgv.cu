@@ -242,7 +242,13 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   X(114, reg, 4, 64, 16, 512)        \
   X(124, reg, 4, 32, 16, 256)        \
   X(134, reg, 4, 32, 32, 1024)       \
-  X(122, reg, 2, 32, 16, 256)
+  X(122, reg, 2, 32, 16, 256)        \
+  X(162, reg, 2, 16, 16, 256)        \
+  X(164, reg, 4, 16, 16, 256)        \
+  X(166, reg, 3, 16, 16, 256)        \
+  X(182, reg, 2, 16, 8, 128)         \
+  X(184, reg, 4, 16, 8, 128)         \
+  X(192, reg, 2, 8, 8, 64)
 
 }  // namespace
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "vfs_kernels.cuh"
 #include "vfs_pixel.cuh"
 
 namespace vfs {
@@ -37,5 +38,16 @@ int tgv_max_iters_per_launch(int variant);
 cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& out, const TgvConsts& c,
                              const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
                              cudaStream_t s);
+
+// Cluster-resident solve of a whole level (vfs_tgv_cluster.cu): all `niter`
+// iterations, then median filter and clamped flow update, in one launch of a
+// `cluster`-CTA cluster.  tgv_cluster_size returns the cluster size to use for
+// an h x w level (0 if the level does not fit); tgv_cluster_prepare sets the
+// kernel attributes and reports the largest cluster the device co-schedules.
+int tgv_cluster_size(int h, int w, int max_cluster);
+cudaError_t tgv_cluster_prepare(int* max_cluster);
+cudaError_t launch_tgv_cluster(int cluster, const TgvState& st, const TgvConsts& c, const float3* sched, int niter,
+                               const SolverConsts& kc, Plane<float2> warp, Plane<float> ubefore,
+                               Plane<const float2> tvec, float limit, int h, int w, cudaStream_t s);
 
 }  // namespace vfs

@@ -45,7 +45,7 @@ class VfsSolveStats(ctypes.Structure):
     """Mirror of ``VfsSolveStats`` in include/vfs_b200.h."""
     _fields_ = [("kernels_per_solve", ctypes.c_longlong), ("tgv_ms", ctypes.c_double),
                 ("tgv_alg_bytes", ctypes.c_double), ("tgv_launches", ctypes.c_longlong),
-                ("tgv_intervals", ctypes.c_int)]
+                ("tgv_intervals", ctypes.c_int), ("tgv_ms_level", ctypes.c_double * 16)]
 
 
 _P = ctypes.c_void_p
@@ -99,6 +99,9 @@ _SIGS = {
     "vfs_static_scratch_bytes": [],
     "vfs_solve_stereo_static": [_PRM, _P, _SZ, _P, _P, _P, _P, _P, _P],
     "vfs_plan_set_timing": [_P, _I],
+    "vfs_plan_set_cluster": [_P, _I],
+    "vfs_plan_set_level_variant": [_P, _I, _I],
+    "vfs_plan_level_cluster": [_P, _I],
     "vfs_plan_stats": [_P, ctypes.POINTER(VfsSolveStats)],
     "vfs_step_schedule": [_I, _D, _P],
 }

@@ -40,9 +40,10 @@ class VFS:
         self._workspace = None
         self._plan_mask = False
         self._plan_fields = False
-        self.tgv_iters_per_launch = 4
+        self.tgv_iters_per_launch = 134
         self.use_graph = False
         self.timing = False
+        self.use_cluster = False
 
     # ---- Python/vfs.py:38-74
     def setup_module(self):
@@ -96,11 +97,14 @@ class VFS:
         call("vfs_plan_set_tgv_variant", plan, int(self.tgv_iters_per_launch))
         call("vfs_plan_set_graph", plan, 1 if self.use_graph else 0)
         call("vfs_plan_set_timing", plan, 1 if self.timing else 0)
+        call("vfs_plan_set_cluster", plan, 1 if self.use_cluster else 0)
+        for l, v in enumerate(getattr(self, "level_variants", [])[:self.param.nLevel]):
+            call("vfs_plan_set_level_variant", plan, l, int(v))
         self._plan, self._plan_key = plan, key
         self._plan_mask = self._plan_fields = False
         return plan
 
-    def configure(self, iters_per_launch=None, use_graph=None, timing=None):
+    def configure(self, iters_per_launch=None, use_graph=None, timing=None, cluster=None):
         """Fused-path options: TGV iterations per launch (1, 2, 4), CUDA-graph
         replay of the whole solve, and TGV event timing (see ``solve_stats``)."""
         if iters_per_launch is not None:
@@ -109,17 +113,36 @@ class VFS:
             self.use_graph = bool(use_graph)
         if timing is not None:
             self.timing = bool(timing)
+        if cluster is not None:
+            self.use_cluster = bool(cluster)
         if self._plan is not None:
             call("vfs_plan_set_tgv_variant", self._plan, int(self.tgv_iters_per_launch))
             call("vfs_plan_set_graph", self._plan, 1 if self.use_graph else 0)
             call("vfs_plan_set_timing", self._plan, 1 if self.timing else 0)
+            call("vfs_plan_set_cluster", self._plan, 1 if self.use_cluster else 0)
+
+    def set_level_variants(self, choice):
+        """Per-level TGV kernel ids, finest level first (0: the default kernel,
+        1000: the cluster-resident kernel)."""
+        self.level_variants = list(choice)
+        if self._plan is not None:
+            for l, v in enumerate(self.level_variants):
+                call("vfs_plan_set_level_variant", self._plan, l, int(v))
+
+    def autotune(self, img_ref, img_other, **kw):
+        """Times every TGV kernel on this plan's levels and keeps the fastest
+        per level (results are bit-identical whichever kernel runs)."""
+        from .autotune import autotune
+        return autotune(self, _dev(img_ref, torch.uint8), _dev(img_other, torch.uint8), **kw)
 
     def solve_stats(self) -> dict:
         """Statistics of the last fused solve (synchronises the current stream)."""
         torch.cuda.current_stream().synchronize()
         st = _lib.VfsSolveStats()
         call("vfs_plan_stats", self._plan, ctypes.byref(st))
-        return {k: getattr(st, k) for k, _ in st._fields_}
+        out = {k: getattr(st, k) for k, _ in st._fields_}
+        out["tgv_ms_level"] = list(st.tgv_ms_level)[:self.param.nLevel]
+        return out
 
     def release(self):
         """Frees the plan (and its workspace)."""
