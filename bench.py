@@ -410,8 +410,25 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small case for ncu: the 800x800 finest level only, 1 warp, 20 TGV iterations, "
+                         "kernel --iters-per-launch everywhere, no graph; two solves, no JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
+    if args.profile_case:
+        torch.cuda.set_device(0)
+        p = params()
+        p.nLevel, p.nWarpIters, p.nSolverIters = 1, 1, 20
+        pair = make_inputs(0)
+        vfs, _ = setup_b200(pair, p)
+        vfs.configure(iters_per_launch=args.iters_per_launch, use_graph=False, timing=False)
+        ref_d = torch.as_tensor(pair.img_ref).cuda()
+        oth_d = torch.as_tensor(pair.img_other).cuda()
+        for _ in range(2):
+            vfs.solve_stereo(ref_d, oth_d)
+        torch.cuda.synchronize()
+        print("profile case done")
+        return
     n, rank, local = dist_init()
     if args.impl == "reference":
         if rank == 0:

@@ -177,6 +177,33 @@ typedef struct VfsSolveStats {
 } VfsSolveStats;
 /* Statistics of the last solve; synchronise its stream first. */
 VFS_API int vfs_plan_stats(VfsPlan* plan, VfsSolveStats* out);
+/* ---- batched solve of many pairs ------------------------------------------
+ * No counterpart in the reference (one pair per solve_stereo call).  Pairs of
+ * uneven resolution share the solver parameters (prm's width/height are
+ * ignored; heights[i] x widths[i] is pair i).  The pairs advance level by
+ * level in lockstep and every TGV pass is one launch over the tiles of all
+ * pairs; per pair the result is bit-identical to vfs_plan_solve.  The caller
+ * provides one workspace of vfs_batch_workspace_size() bytes. */
+typedef struct VfsBatch VfsBatch;
+VFS_API int vfs_batch_workspace_size(const VfsParams* prm, int n, const int* heights, const int* widths,
+                                     size_t* bytes);
+VFS_API int vfs_batch_create(const VfsParams* prm, int n, const int* heights, const int* widths, void* workspace,
+                             size_t workspace_bytes, VfsBatch** batch_out);
+VFS_API int vfs_batch_destroy(VfsBatch* batch);
+/* mask (u8, pitch bytes), tvf and cvf (H, W, 2) of pair i */
+VFS_API int vfs_batch_set_pair(VfsBatch* batch, int i, const uint8_t* mask, size_t mask_pitch, const float* tvf_hw2,
+                               const float* cvf_hw2, void* stream);
+/* host arrays of n device pointers each */
+VFS_API int vfs_batch_solve(VfsBatch* batch, const uint8_t* const* img_refs, const uint8_t* const* img_others,
+                            float* const* warps_out_hw2, void* stream);
+VFS_API int vfs_batch_triangulate(VfsBatch* batch, int i, float f, float u0, float v0, const float* t,
+                                  float* xyz_out_hw3, void* stream);
+/* per-level TGV kernel of the batched launches (a 1xx register-owned variant) */
+VFS_API int vfs_batch_set_level_variant(VfsBatch* batch, int level, int variant);
+VFS_API int vfs_batch_set_graph(VfsBatch* batch, int enable);
+VFS_API int vfs_batch_set_timing(VfsBatch* batch, int enable);
+VFS_API int vfs_batch_stats(VfsBatch* batch, VfsSolveStats* out);
+
 /* ---- whole solve with no device allocation --------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (a real-time loop with a fixed memory budget, a host callback, a foreign

@@ -82,14 +82,30 @@ __device__ __forceinline__ void dual_px(uint8_t code, float uc, float2 vc, float
   }
   const float2 tu = make_float2(fmaf(abc.x, gradU.x, abc.z * gradU.y), fmaf(abc.z, gradU.x, abc.y * gradU.y));
   const float2 up = make_float2(fmaf(scaleP, tu.x, p->x), fmaf(scaleP, tu.y, p->y));
-  float norm = fmaxf(hypotf(up.x, up.y), 1.0f);
-  const float2 pn = make_float2(up.x / norm, up.y / norm);
+  // Projection onto the unit ball: norm = max(|up|, 1), p = up / norm.  When
+  // the L1 norm is <= 0.99 the Euclidean norm (and hypotf's result, accurate
+  // to a few ulp) is below 1, so norm is exactly 1 and up / 1 == up: the
+  // shortcut skips hypotf and the divisions with bit-identical results.  The
+  // same holds when norm comes out exactly 1 (NaNs take the full path).
+  float2 pn;
+  if (fabsf(up.x) + fabsf(up.y) <= 0.99f) {
+    pn = up;
+  } else {
+    const float norm = fmaxf(hypotf(up.x, up.y), 1.0f);
+    pn = (norm == 1.0f && up.x == up.x && up.y == up.y) ? up : make_float2(up.x / norm, up.y / norm);
+  }
   *p = pn;
   *tp = make_float2(fmaf(abc.x, pn.x, abc.z * pn.y), fmaf(abc.z, pn.x, abc.y * pn.y));
   const float4 uq = make_float4(fmaf(scaleQ, gradV.x, q->x), fmaf(scaleQ, gradV.y, q->y),
                                 fmaf(scaleQ, gradV.z, q->z), fmaf(scaleQ, gradV.w, q->w));
-  norm = fmaxf(norm4df(uq.x, uq.y, uq.z, uq.w), 1.0f);
-  *q = make_float4(uq.x / norm, uq.y / norm, uq.z / norm, uq.w / norm);
+  if (fabsf(uq.x) + fabsf(uq.y) + fabsf(uq.z) + fabsf(uq.w) <= 0.99f) {
+    *q = uq;
+  } else {
+    const float norm = fmaxf(norm4df(uq.x, uq.y, uq.z, uq.w), 1.0f);
+    *q = (norm == 1.0f && uq.x == uq.x && uq.y == uq.y && uq.z == uq.z && uq.w == uq.w)
+             ? uq
+             : make_float4(uq.x / norm, uq.y / norm, uq.z / norm, uq.w / norm);
+  }
 }
 
 // ---------------------------------------------------------------- K11 threshold

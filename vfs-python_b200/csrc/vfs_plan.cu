@@ -7,10 +7,8 @@
 #include <new>
 #include <vector>
 
-#include "vfs_api_util.cuh"
-#include "vfs_kernels.cuh"
+#include "vfs_plan_impl.cuh"
 #include "vfs_sample.cuh"
-#include "vfs_tgv.cuh"
 
 namespace vfs {
 namespace {
@@ -83,61 +81,6 @@ __global__ void k_derivs_init(TgvConsts out, TgvState st, Plane<const float> ube
 
 using namespace vfs;
 
-struct VfsPlan {
-  VfsParams prm;
-  SolverConsts kc;
-  int L = 0;
-  struct Level {
-    int h, w;
-    Plane<float> ref, other;
-    Plane<float2> tvf;
-    Plane<uint8_t> mask;
-    uint8_t* code;
-    cudaTextureObject_t ref_tex = 0, other_tex = 0, tvf_tex = 0, mask_tex = 0, smooth_tex = 0, warped_tex = 0,
-                        ubefore_tex = 0, warp_tex = 0;
-  };
-  std::vector<Level> lv;
-  Plane<float> other0;
-  cudaTextureObject_t other0_tex = 0;
-  Plane<float2> calib;
-  Plane<float> smooth, warped;
-  Plane<float2> tvec;
-  TgvConsts cst;
-  float* cplanes[8];
-  TgvState st[2];
-  Plane<float> ubefore[2];
-  Plane<float2> warp[2];
-  float3* sched = nullptr;
-  int variant = 134;
-  int level_variant[32] = {0};  // 0: the plan's variant; VFS_TGV_CLUSTER: cluster kernel
-  bool mask_set = false, fields_set = false, solved = false;
-  std::vector<cudaTextureObject_t> textures;
-  // input staging (workspace), so a captured graph has fixed pointers
-  uint8_t* stage_ref = nullptr;
-  uint8_t* stage_other = nullptr;
-  // graph replay
-  bool use_graph = false;
-  cudaStream_t gstream = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-  // instrumentation: an event pair around each warp's TGV launches
-  bool timing = false;
-  std::vector<cudaEvent_t> tev;
-  std::vector<double> tev_bytes;
-  std::vector<long long> tev_launches;
-  int tev_used = 0;
-  std::vector<int> tev_level;
-  long long kernels_per_solve = 0;
-  // cluster-resident solve for levels that fit one cluster
-  bool use_cluster = false;
-  int max_cluster = 0;
-
-  void drop_graph() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    gexec = nullptr;
-  }
-};
-
 namespace {
 
 int make_tex(VfsPlan* pl, const void* ptr, int h, int w, size_t pitch, int kind, int linear, cudaTextureObject_t* out) {
@@ -197,130 +140,191 @@ void init_levels(VfsPlan* pl) {
   }
 }
 
-// Enqueues one complete solve on `s` from the staged images into warp[0].
-int enqueue_solve(VfsPlan* pl, cudaStream_t s) {
+}  // namespace
+
+namespace vfs {
+
+// create_image_pyramid, Python/vfs.py:121-157, from the staged images.
+int plan_pyramids(VfsPlan* pl, cudaStream_t s, long long* nk) {
   const int L = pl->L;
   auto& v0 = pl->lv[0];
-  const SolverConsts& kc = pl->kc;
-  long long nk = 0;
-  pl->tev_used = 0;
-  // create_image_pyramid, Python/vfs.py:121-157
   VFS_TRY_CUDA(launch_cast_and_scale(v0.ref, {pl->stage_ref, (size_t)v0.w}, v0.h, v0.w, s), "castAndScale");
   VFS_TRY_CUDA(launch_cast_and_scale(pl->other0, {pl->stage_other, (size_t)v0.w}, v0.h, v0.w, s), "castAndScale");
-  nk += 2;
-  for (int l = 1; l < L; ++l, ++nk)
+  *nk += 2;
+  for (int l = 1; l < L; ++l, ++*nk)
     VFS_TRY_CUDA(launch_downsample_image(pl->lv[l].ref, pl->lv[l - 1].ref_tex, pl->lv[l].h, pl->lv[l].w, s),
                  "downSamplingImage");
   VFS_TRY_CUDA(launch_warp_image(v0.other, {pl->calib.ptr, pl->calib.pitch}, pl->other0_tex, v0.h, v0.w, s),
                "warpingImage");
-  ++nk;
-  for (int l = 1; l < L; ++l, ++nk)
+  ++*nk;
+  for (int l = 1; l < L; ++l, ++*nk)
     VFS_TRY_CUDA(launch_downsample_image(pl->lv[l].other, pl->lv[l - 1].other_tex, pl->lv[l].h, pl->lv[l].w, s),
                  "downSamplingImage");
+  return VFS_OK;
+}
 
-  const int nIt = pl->prm.nSolverIters;
-  for (int l = L - 1; l >= 0; --l) {
-    auto& v = pl->lv[l];
-    const int h = v.h, w = v.w, b = l % 2;
-    const dim3 g = grid2d(h, w), blk(kBX, kBY);
-    // TGV kernel for this level: the plan's variant, a per-level choice (the
-    // autotuner's), or the cluster-resident kernel where the level fits
-    int var = pl->level_variant[l] ? pl->level_variant[l] : pl->variant;
-    int cs = 0;
-    if (var == VFS_TGV_CLUSTER || (pl->level_variant[l] == 0 && pl->use_cluster)) {
-      cs = tgv_cluster_size(h, w, pl->max_cluster);
-      if (var == VFS_TGV_CLUSTER) var = pl->variant;
-    }
-    const int K = tgv_max_iters_per_launch(var);
-    const int npass = (nIt + K - 1) / K;
-    if (l == L - 1) {  // warpUV, u, u_ <- 0 (Python/vfs.py:466-469)
-      VFS_TRY_CUDA(cudaMemset2DAsync(pl->ubefore[b].ptr, pl->ubefore[b].pitch, 0, (size_t)w * 4, h, s), "memset");
-      VFS_TRY_CUDA(cudaMemset2DAsync(pl->warp[b].ptr, pl->warp[b].pitch, 0, (size_t)w * 8, h, s), "memset");
-    }
-    Plane<const float> ub_src{pl->ubefore[b].ptr, pl->ubefore[b].pitch};
-    Plane<const uint8_t> mask{v.mask.ptr, v.mask.pitch};
-    // gaussian + computeTensorEtaMasked, Python/vfs.py:474-475
-    VFS_TRY_CUDA(launch_gaussian_masked(pl->smooth, v.ref_tex, mask, h, w, s), "gaussianMasked");
-    TgvConsts cst = pl->cst;
-    cst.code = v.code;
-    k_tensor_soa<<<g, blk, 0, s>>>(cst, v.code, v.smooth_tex, mask, kc, h, w);
-    VFS_TRY_CUDA(cudaGetLastError(), "tensor");
-    nk += 2;
-    for (int wi = 0; wi < pl->prm.nWarpIters; ++wi) {
-      // findWarpingVector + warpingImage, Python/vfs.py:480-483
-      VFS_TRY_CUDA(launch_warp_prologue(Plane<float2>{pl->tvec.ptr, (size_t)w * 8}, pl->warped,
-                                        {pl->warp[b].ptr, pl->warp[b].pitch}, v.tvf_tex, v.other_tex, h, w, s),
-                   "warp prologue");
-      // computeDerivatives + solver reset, Python/vfs.py:486-497
-      k_derivs_init<<<g, blk, 0, s>>>(cst, pl->st[0], {pl->ubefore[b].ptr, pl->ubefore[b].pitch}, ub_src, v.ref_tex,
-                                      v.warped_tex, v.tvf_tex, h, w);
-      VFS_TRY_CUDA(cudaGetLastError(), "derivatives");
-      nk += 2;
-      // solver iterations, Python/vfs.py:498-515
-      const int launches = cs > 0 ? 1 : npass;
-      const bool timed = pl->timing && launches > 0;
-      if (timed) {
-        const int pair = pl->tev_used;
-        while ((int)pl->tev.size() < 2 * (pair + 1)) {
-          cudaEvent_t e;
-          VFS_TRY_CUDA(cudaEventCreate(&e), "event create");
-          pl->tev.push_back(e);
-        }
-        if ((int)pl->tev_bytes.size() < pair + 1) {
-          pl->tev_bytes.resize(pair + 1);
-          pl->tev_launches.resize(pair + 1);
-          pl->tev_level.resize(pair + 1);
-        }
-        VFS_TRY_CUDA(cudaEventRecordWithFlags(pl->tev[2 * pair], s, cudaEventRecordExternal), "event record");
-      }
-      if (cs > 0) {
-        // the whole level in one cluster: iterations + median + clamp
-        VFS_TRY_CUDA(launch_tgv_cluster(cs, pl->st[0], cst, pl->sched, nIt, kc, {pl->warp[b].ptr, pl->warp[b].pitch},
-                                        pl->ubefore[b], {pl->tvec.ptr, (size_t)w * 8}, kc.upperLimit, h, w, s),
-                     "tgv cluster");
-        ++nk;
-      } else {
-        for (int j = 0; j < npass; ++j) {
-          const int it0 = j * K;
-          VFS_TRY_CUDA(launch_tgv_block(var, pl->st[j % 2], pl->st[(j + 1) % 2], cst, pl->sched, it0,
-                                        std::min(K, nIt - it0), kc, h, w, s),
-                       "tgv");
-        }
-        nk += npass;
-      }
-      if (timed) {
-        const int pair = pl->tev_used++;
-        VFS_TRY_CUDA(cudaEventRecordWithFlags(pl->tev[2 * pair + 1], s, cudaEventRecordExternal), "event record");
-        // algorithmic bytes: 113 per pixel per iteration (state in and out,
-        // per-warp constants in)
-        pl->tev_bytes[pair] = 113.0 * (double)h * w * nIt;
-        pl->tev_launches[pair] = launches;
-        pl->tev_level[pair] = l;
-      }
-      if (cs > 0) {
-        ub_src = {pl->st[0].ub, (size_t)w * 4};
-      } else {
-        const TgvState& fin = pl->st[npass % 2];
-        // medianFilter + computeOpticalFlowWithClamp, Python/vfs.py:518-521
-        VFS_TRY_CUDA(launch_median_clamp({pl->warp[b].ptr, pl->warp[b].pitch}, pl->ubefore[b],
-                                         {fin.u, (size_t)w * 4}, {pl->tvec.ptr, (size_t)w * 8}, mask, kc.upperLimit,
-                                         h, w, s),
-                     "median/clamp");
-        ++nk;
-        ub_src = {fin.ub, (size_t)w * 4};
-      }
-    }
-    if (l > 0) {  // Python/vfs.py:523-528
-      auto& f = pl->lv[l - 1];
-      const int nb = (l - 1) % 2;
-      VFS_TRY_CUDA(launch_upsample1(pl->ubefore[nb], v.ubefore_tex, kc.fscale, f.h, f.w, s), "upSampling1");
-      VFS_TRY_CUDA(launch_upsample2(pl->warp[nb], v.warp_tex, kc.fscale, f.h, f.w, s), "upSampling");
-      nk += 2;
-    }
+// Start of a level: kernel choice, the coarsest level's zero state
+// (Python/vfs.py:466-469), gaussian + tensor (Python/vfs.py:474-475).
+int plan_level_begin(VfsPlan* pl, int l, LevelCtx* c, cudaStream_t s, long long* nk) {
+  auto& v = pl->lv[l];
+  c->l = l;
+  c->h = v.h;
+  c->w = v.w;
+  c->b = l % 2;
+  // TGV kernel for this level: the plan's variant, a per-level choice (the
+  // autotuner's), or the cluster-resident kernel where the level fits
+  int var = pl->level_variant[l] ? pl->level_variant[l] : pl->variant;
+  int cs = 0;
+  if (var == VFS_TGV_CLUSTER || (pl->level_variant[l] == 0 && pl->use_cluster)) {
+    cs = tgv_cluster_size(v.h, v.w, pl->max_cluster);
+    if (var == VFS_TGV_CLUSTER) var = pl->variant;
   }
-  // warpUV_ref[masks[0] == 0, :] = 0, Python/vfs.py:531
+  c->var = var;
+  c->cs = cs;
+  c->K = tgv_max_iters_per_launch(var);
+  c->npass = (pl->prm.nSolverIters + c->K - 1) / c->K;
+  const int h = v.h, w = v.w, b = c->b;
+  if (l == pl->L - 1) {
+    VFS_TRY_CUDA(cudaMemset2DAsync(pl->ubefore[b].ptr, pl->ubefore[b].pitch, 0, (size_t)w * 4, h, s), "memset");
+    VFS_TRY_CUDA(cudaMemset2DAsync(pl->warp[b].ptr, pl->warp[b].pitch, 0, (size_t)w * 8, h, s), "memset");
+  }
+  c->ub_src = {pl->ubefore[b].ptr, pl->ubefore[b].pitch};
+  c->mask = {v.mask.ptr, v.mask.pitch};
+  VFS_TRY_CUDA(launch_gaussian_masked(pl->smooth, v.ref_tex, c->mask, h, w, s), "gaussianMasked");
+  c->cst = pl->cst;
+  c->cst.code = v.code;
+  k_tensor_soa<<<grid2d(h, w), dim3(kBX, kBY), 0, s>>>(c->cst, v.code, v.smooth_tex, c->mask, pl->kc, h, w);
+  VFS_TRY_CUDA(cudaGetLastError(), "tensor");
+  *nk += 2;
+  return VFS_OK;
+}
+
+// findWarpingVector + warpingImage (Python/vfs.py:480-483), then
+// computeDerivatives + the solver reset (Python/vfs.py:486-497) into st[0].
+int plan_warp_pre(VfsPlan* pl, LevelCtx* c, cudaStream_t s, long long* nk) {
+  auto& v = pl->lv[c->l];
+  const int h = c->h, w = c->w, b = c->b;
+  VFS_TRY_CUDA(launch_warp_prologue(Plane<float2>{pl->tvec.ptr, (size_t)w * 8}, pl->warped,
+                                    {pl->warp[b].ptr, pl->warp[b].pitch}, v.tvf_tex, v.other_tex, h, w, s),
+               "warp prologue");
+  k_derivs_init<<<grid2d(h, w), dim3(kBX, kBY), 0, s>>>(c->cst, pl->st[0], {pl->ubefore[b].ptr, pl->ubefore[b].pitch},
+                                                        c->ub_src, v.ref_tex, v.warped_tex, v.tvf_tex, h, w);
+  VFS_TRY_CUDA(cudaGetLastError(), "derivatives");
+  *nk += 2;
+  return VFS_OK;
+}
+
+// The solver iterations of one warp (Python/vfs.py:498-515), with optional
+// timing events around them.
+int plan_warp_tgv(VfsPlan* pl, LevelCtx* c, cudaStream_t s, long long* nk, unsigned ev_flags) {
+  const int h = c->h, w = c->w, b = c->b;
+  const int nIt = pl->prm.nSolverIters;
+  const int launches = c->cs > 0 ? 1 : c->npass;
+  const bool timed = pl->timing && launches > 0;
+  int pair = -1;
+  if (timed) {
+    pair = pl->tev_used++;
+    while ((int)pl->tev.size() < 2 * (pair + 1)) {
+      cudaEvent_t e;
+      VFS_TRY_CUDA(cudaEventCreate(&e), "event create");
+      pl->tev.push_back(e);
+    }
+    if ((int)pl->tev_bytes.size() < pair + 1) {
+      pl->tev_bytes.resize(pair + 1);
+      pl->tev_launches.resize(pair + 1);
+      pl->tev_level.resize(pair + 1);
+    }
+    VFS_TRY_CUDA(cudaEventRecordWithFlags(pl->tev[2 * pair], s, ev_flags), "event record");
+  }
+  if (c->cs > 0) {
+    // the whole level in one cluster: iterations + median + clamp
+    VFS_TRY_CUDA(launch_tgv_cluster(c->cs, pl->st[0], c->cst, pl->sched, nIt, pl->kc,
+                                    {pl->warp[b].ptr, pl->warp[b].pitch}, pl->ubefore[b],
+                                    {pl->tvec.ptr, (size_t)w * 8}, pl->kc.upperLimit, h, w, s),
+                 "tgv cluster");
+    ++*nk;
+  } else {
+    for (int j = 0; j < c->npass; ++j) {
+      const int it0 = j * c->K;
+      VFS_TRY_CUDA(launch_tgv_block(c->var, pl->st[j % 2], pl->st[(j + 1) % 2], c->cst, pl->sched, it0,
+                                    std::min(c->K, nIt - it0), pl->kc, h, w, s),
+                   "tgv");
+    }
+    *nk += c->npass;
+  }
+  if (timed) {
+    VFS_TRY_CUDA(cudaEventRecordWithFlags(pl->tev[2 * pair + 1], s, ev_flags), "event record");
+    // algorithmic bytes: 113 per pixel per iteration (state in and out,
+    // per-warp constants in)
+    pl->tev_bytes[pair] = 113.0 * (double)h * w * nIt;
+    pl->tev_launches[pair] = launches;
+    pl->tev_level[pair] = c->l;
+  }
+  return VFS_OK;
+}
+
+// medianFilter + computeOpticalFlowWithClamp (Python/vfs.py:518-521); the
+// cluster kernel does them itself.
+int plan_warp_post(VfsPlan* pl, LevelCtx* c, cudaStream_t s, long long* nk) {
+  const int h = c->h, w = c->w, b = c->b;
+  if (c->cs > 0) {
+    c->ub_src = {pl->st[0].ub, (size_t)w * 4};
+    return VFS_OK;
+  }
+  const TgvState& fin = pl->st[c->npass % 2];
+  VFS_TRY_CUDA(launch_median_clamp({pl->warp[b].ptr, pl->warp[b].pitch}, pl->ubefore[b], {fin.u, (size_t)w * 4},
+                                   {pl->tvec.ptr, (size_t)w * 8}, c->mask, pl->kc.upperLimit, h, w, s),
+               "median/clamp");
+  ++*nk;
+  c->ub_src = {fin.ub, (size_t)w * 4};
+  return VFS_OK;
+}
+
+// Up-sampling to the next finer level, Python/vfs.py:523-528.
+int plan_level_end(VfsPlan* pl, LevelCtx* c, cudaStream_t s, long long* nk) {
+  const int l = c->l;
+  if (l == 0) return VFS_OK;
+  auto& v = pl->lv[l];
+  auto& f = pl->lv[l - 1];
+  const int nb = (l - 1) % 2;
+  VFS_TRY_CUDA(launch_upsample1(pl->ubefore[nb], v.ubefore_tex, pl->kc.fscale, f.h, f.w, s), "upSampling1");
+  VFS_TRY_CUDA(launch_upsample2(pl->warp[nb], v.warp_tex, pl->kc.fscale, f.h, f.w, s), "upSampling");
+  *nk += 2;
+  return VFS_OK;
+}
+
+// warpUV_ref[masks[0] == 0, :] = 0, Python/vfs.py:531.
+int plan_finish(VfsPlan* pl, cudaStream_t s, long long* nk) {
+  auto& v0 = pl->lv[0];
   VFS_TRY_CUDA(launch_mask_flow(pl->warp[0], {v0.mask.ptr, v0.mask.pitch}, v0.h, v0.w, s), "mask flow");
-  ++nk;
+  ++*nk;
+  return VFS_OK;
+}
+
+}  // namespace vfs
+
+namespace {
+
+// Enqueues one complete solve on `s` from the staged images into warp[0].
+int enqueue_solve(VfsPlan* pl, cudaStream_t s) {
+  long long nk = 0;
+  pl->tev_used = 0;
+  // timing events: external event nodes when captured into a graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  VFS_TRY_CUDA(cudaStreamIsCapturing(s, &cap), "capture status");
+  const unsigned ev_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+  VFS_TRY(plan_pyramids(pl, s, &nk));
+  for (int l = pl->L - 1; l >= 0; --l) {
+    LevelCtx c;
+    VFS_TRY(plan_level_begin(pl, l, &c, s, &nk));
+    for (int wi = 0; wi < pl->prm.nWarpIters; ++wi) {
+      VFS_TRY(plan_warp_pre(pl, &c, s, &nk));
+      VFS_TRY(plan_warp_tgv(pl, &c, s, &nk, ev_flags));
+      VFS_TRY(plan_warp_post(pl, &c, s, &nk));
+    }
+    VFS_TRY(plan_level_end(pl, &c, s, &nk));
+  }
+  VFS_TRY(plan_finish(pl, s, &nk));
   pl->kernels_per_solve = nk;
   return VFS_OK;
 }

@@ -27,6 +27,7 @@
 // Per-pixel arithmetic is vfs_pixel.cuh's, shared with the one-kernel-per-
 // step entry points, so the fused solver is bit-identical to them.
 #include <cstdio>
+#include <string>
 
 #include "vfs_tgv.cuh"
 
@@ -208,8 +209,25 @@ cudaError_t prepare_block() {
 
 template <int K, int TX, int TY, int NT>
 cudaError_t prepare_reg() {
-  return cudaFuncSetAttribute(k_tgv_reg<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_tgv_reg<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)RegGeom<K, TX, TY>::smem_bytes());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tgv_reg_batch<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)RegGeom<K, TX, TY>::smem_bytes());
+}
+
+template <int K, int TX, int TY, int NT>
+cudaError_t batch_reg(const TgvBatchItem* items, int n_items, int total_tiles, int parity, const float3* sched,
+                      int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
+  k_tgv_reg_batch<K, TX, TY, NT><<<total_tiles, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(items, n_items, parity,
+                                                                                            sched, it0, niter, kc);
+  return cudaGetLastError();
+}
+
+template <int K, int TX, int TY, int NT>
+cudaError_t batch_block(const TgvBatchItem*, int, int, int, const float3*, int, int, const SolverConsts&,
+                        cudaStream_t) {
+  return cudaErrorInvalidValue;  // batched launches use the register-owned kernels
 }
 
 template <int K, int TX, int TY, int NT>
@@ -279,6 +297,31 @@ int tgv_variant_list(int* ids, int cap) {
   VFS_TGV_VARIANTS(VFS_LIST)
 #undef VFS_LIST
   return n;
+}
+
+bool tgv_tile_shape(int variant, int* tx, int* ty) {
+  switch (variant) {
+#define VFS_SHAPE(id, impl, K, TX, TY, NT) \
+  case id:                                \
+    *tx = TX;                             \
+    *ty = TY;                             \
+    return std::string(#impl) == "reg";
+    VFS_TGV_VARIANTS(VFS_SHAPE)
+#undef VFS_SHAPE
+    default: return false;
+  }
+}
+
+cudaError_t launch_tgv_batch(int variant, const TgvBatchItem* items, int n_items, int total_tiles, int parity,
+                             const float3* sched, int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
+  if (n_items <= 0 || total_tiles <= 0 || niter <= 0) return cudaSuccess;
+  switch (variant) {
+#define VFS_BATCH_V(id, impl, K, TX, TY, NT) \
+  case id: return batch_##impl<K, TX, TY, NT>(items, n_items, total_tiles, parity, sched, it0, niter, kc, s);
+    VFS_TGV_VARIANTS(VFS_BATCH_V)
+#undef VFS_BATCH_V
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& out, const TgvConsts& c,

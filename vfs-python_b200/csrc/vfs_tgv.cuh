@@ -24,6 +24,22 @@ struct TgvConsts {
   const uint8_t* code;
 };
 
+// One image of a batched TGV launch: its two state sets (ping-pong), its
+// per-warp constants, its size and where its tiles start in the launch.
+struct TgvBatchItem {
+  TgvState st[2];
+  TgvConsts cst;
+  int h, w, tiles_x, tile_base;
+};
+
+// Tile shape of a register-owned variant (false for other variants).
+bool tgv_tile_shape(int variant, int* tx, int* ty);
+
+// Batched launch of a register-owned variant over `total_tiles` blocks: the
+// items (in device memory) read st[parity] and write st[parity ^ 1].
+cudaError_t launch_tgv_batch(int variant, const TgvBatchItem* items, int n_items, int total_tiles, int parity,
+                             const float3* sched, int it0, int niter, const SolverConsts& kc, cudaStream_t s);
+
 // Sets the kernels' shared-memory attributes (call before any graph capture).
 cudaError_t tgv_prepare();
 

@@ -24,10 +24,11 @@ struct RegGeom {
   static constexpr size_t smem_bytes() { return (size_t)kRegPlanes * N * sizeof(float); }
 };
 
+// One CTA's tile whose origin is (x0, y0).
 template <int K, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1)) k_tgv_reg(TgvState in, TgvState out, TgvConsts cst,
-                                                   const float3* __restrict__ sched, int it0, int niter,
-                                                   SolverConsts kc, int h, int w) {
+__device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState& out, const TgvConsts& cst,
+                                             const float3* __restrict__ sched, int it0, int niter,
+                                             const SolverConsts& kc, int h, int w, int x0, int y0) {
   using G = RegGeom<K, TX, TY>;
   constexpr int WX = G::WX, N = G::N, J = (N + NT - 1) / NT;
   extern __shared__ float4 smem_raw[];
@@ -42,7 +43,6 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1)) k_tgv_reg(TgvState in
   float* const sQZ = sm + rQZ * N;
   float* const sQW = sm + rQW * N;
 
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const long n = (long)h * w;
   const long base = (long)(y0 - 2 * K) * w + (x0 - 2 * K);
 
@@ -169,6 +169,34 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1)) k_tgv_reg(TgvState in
     out.qz[f] = sQZ[i];
     out.qw[f] = sQW[i];
   }
+}
+
+template <int K, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
+    k_tgv_reg(TgvState in, TgvState out, TgvConsts cst, const float3* __restrict__ sched, int it0, int niter,
+              SolverConsts kc, int h, int w) {
+  tgv_reg_tile<K, TX, TY, NT>(in, out, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY);
+}
+
+// Batched: one launch over the tiles of many images (the pairs of a batch at
+// the same pyramid level and pass).  items[i].tile_base is the first block of
+// item i; block b belongs to the last item whose tile_base <= b.
+template <int K, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
+    k_tgv_reg_batch(const TgvBatchItem* __restrict__ items, int n_items, int parity,
+                    const float3* __restrict__ sched, int it0, int niter, SolverConsts kc) {
+  int lo = 0, hi = n_items - 1;
+  const int bid = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].tile_base <= bid) lo = mid;
+    else hi = mid - 1;
+  }
+  const TgvBatchItem& it = items[lo];
+  const int t = bid - it.tile_base;
+  const int ty = t / it.tiles_x, tx = t - ty * it.tiles_x;
+  tgv_reg_tile<K, TX, TY, NT>(it.st[parity], it.st[parity ^ 1], it.cst, sched, it0, niter, kc, it.h, it.w, tx * TX,
+                              ty * TY);
 }
 
 }  // namespace

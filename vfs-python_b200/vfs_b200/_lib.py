@@ -97,6 +97,16 @@ _SIGS = {
     "vfs_plan_set_graph": [_P, _I],
     "vfs_tgv_variants": [_P, _I, _P],
     "vfs_static_scratch_bytes": [],
+    "vfs_batch_workspace_size": [_PRM, _I, _P, _P, ctypes.POINTER(_SZ)],
+    "vfs_batch_create": [_PRM, _I, _P, _P, _P, _SZ, ctypes.POINTER(_P)],
+    "vfs_batch_destroy": [_P],
+    "vfs_batch_set_pair": [_P, _I, _P, _SZ, _P, _P, _P],
+    "vfs_batch_solve": [_P, _P, _P, _P, _P],
+    "vfs_batch_triangulate": [_P, _I, _F, _F, _F, _P, _P, _P],
+    "vfs_batch_set_level_variant": [_P, _I, _I],
+    "vfs_batch_set_graph": [_P, _I],
+    "vfs_batch_set_timing": [_P, _I],
+    "vfs_batch_stats": [_P, ctypes.POINTER(VfsSolveStats)],
     "vfs_solve_stereo_static": [_PRM, _P, _SZ, _P, _P, _P, _P, _P, _P],
     "vfs_plan_set_timing": [_P, _I],
     "vfs_plan_set_cluster": [_P, _I],
