@@ -350,6 +350,85 @@ def run_b200(args, n, rank, local):
     return line
 
 
+def _batched_pair(args):
+    """One pair of the batched workload (process-pool worker)."""
+    import os as _os
+    import sys as _sys
+    _sys.path[:0] = [ROOT, _os.path.join(ROOT, "vfs-python_b200")]
+    from vfs_b200.synthetic import make_pair
+    size, t, seed = args
+    return make_pair(size, t, seed=seed, n_level=4)
+
+
+def batched_workload(n_pairs=32, seed=0):
+    """Sizes drawn from {480, 640, 800, 1024}, translation direction uniform on
+    the sphere with magnitude in [0.05, 0.2] m, per-pair seeds."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice([480, 640, 800, 1024], size=n_pairs)
+    out = []
+    for i in range(n_pairs):
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        out.append((int(sizes[i]), tuple(d * rng.uniform(0.05, 0.2)), i))
+    return out
+
+
+def run_batched(args, n, rank, local):
+    """32 pairs of uneven resolution, 4 levels x 10 warps x 50 iterations,
+    solved as one batch (one graph, one TGV launch per pass over all pairs)."""
+    import multiprocessing as mpc
+    from vfs_b200.batch import VFSBatch
+    from vfs_b200.distributed import shard, pair_cost
+    from vfs_b200 import EquidistantCam
+    from vfs_b200.vector_field import get_vector_fields, get_grid_zero
+    work = batched_workload()
+    costs = [pair_cost(s, s, 4, 2.0, 10, 50) for s, _, _ in work]
+    mine = shard(costs, n, rank)
+    with mpc.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        pairs = pool.map(_batched_pair, [work[i] for i in mine])
+    p = params()
+    p.nLevel, p.nWarpIters, p.nSolverIters = 4, 10, 50
+    sizes = [pp.img_ref.shape for pp in pairs]
+    batch = VFSBatch(p, sizes)
+    for i, pp in enumerate(pairs):
+        cam = EquidistantCam(pp.intrinsics)
+        cam.setup_module()
+        tvf, cvf = get_vector_fields(get_grid_zero(pp.img_ref.shape), cam, cam, pp.R, pp.t, 1)
+        batch.set_pair(i, pp.mask, tvf, cvf)
+    refs = [torch.as_tensor(pp.img_ref).cuda() for pp in pairs]
+    oths = [torch.as_tensor(pp.img_other).cuda() for pp in pairs]
+    choice = batch.autotune(refs, oths) if not args.no_autotune else None
+    batch.configure(use_graph=True, timing=True)
+    for _ in range(args.warmup):
+        batch.solve(refs, oths)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    barrier(n)
+    tot = 0.0
+    tgv = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            batch.solve(refs, oths)
+            e1.record()
+            e1.synchronize()
+            tot += e0.elapsed_time(e1) / 1e3
+            tgv += batch.stats()["tgv_ms"] / 1e3
+    barrier(n)
+    t_max = max_over_ranks(tot, n)
+    value = len(work) * args.steps / t_max if n > 1 else len(pairs) * args.steps / t_max
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (per-pair seeds)",
+            "config": {"workload": "batched: 32 pairs, sides from {480, 640, 800, 1024}, random translation "
+                                   "directions, 4 levels x 10 warps x 50 TGV iterations, one batched graph",
+                       "pairs_this_rank": len(pairs), "tgv_kernel_per_level": choice,
+                       "parallelism": f"dp{n} (pairs sharded by cost)",
+                       "l2": "flushed between steps (256 MiB write outside the timed events)"},
+            "tgv_share_of_step": tgv / tot if tot else None, "clocks": clk.summary()}
+
+
 def run_reference(args, n, rank, local):
     from oracle.refgpu import refpath
     p = params()
@@ -408,20 +487,29 @@ def main():
     ap.add_argument("--iters-per-launch", type=int, default=134)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--workload", default="single", choices=["single", "batched"],
+                    help="single: the 800x800 pair (default); batched: 32 uneven pairs in one batch")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu: the 800x800 finest level only, 1 warp, 20 TGV iterations, "
-                         "kernel --iters-per-launch everywhere, no graph; two solves, no JSON line")
+                         "kernel --iters-per-launch everywhere (1000: cluster kernel), no graph; two solves")
+    ap.add_argument("--profile-size", type=int, default=SIZE)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
     if args.profile_case:
         torch.cuda.set_device(0)
         p = params()
         p.nLevel, p.nWarpIters, p.nSolverIters = 1, 1, 20
-        pair = make_inputs(0)
+        from vfs_b200.synthetic import make_pair
+        pair = make_pair(args.profile_size, T, seed=0, n_level=N_LEVEL)
+        p.width = p.height = args.profile_size
         vfs, _ = setup_b200(pair, p)
-        vfs.configure(iters_per_launch=args.iters_per_launch, use_graph=False, timing=False)
+        if args.iters_per_launch == 1000:  # the cluster-resident kernel
+            vfs.configure(use_graph=False, timing=False)
+            vfs.set_level_variants([1000])
+        else:
+            vfs.configure(iters_per_launch=args.iters_per_launch, use_graph=False, timing=False)
         ref_d = torch.as_tensor(pair.img_ref).cuda()
         oth_d = torch.as_tensor(pair.img_other).cuda()
         for _ in range(2):
@@ -433,6 +521,10 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args, n, rank, local)), flush=True)
+    elif args.workload == "batched":
+        line = run_batched(args, n, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     else:
         line = run_b200(args, n, rank, local)
         if rank == 0:

@@ -266,7 +266,29 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   X(166, reg, 3, 16, 16, 256)        \
   X(182, reg, 2, 16, 8, 128)         \
   X(184, reg, 4, 16, 8, 128)         \
-  X(192, reg, 2, 8, 8, 64)
+  X(192, reg, 2, 8, 8, 64)           \
+  X(135, reg, 4, 32, 28, 1024)       \
+  X(136, reg, 4, 32, 24, 1024)       \
+  X(174, reg, 4, 24, 24, 512)        \
+  X(173, reg, 3, 24, 24, 512)        \
+  X(193, reg, 3, 8, 8, 64)           \
+  X(201, reg, 2, 16, 16, 512)        \
+  X(202, reg, 3, 16, 16, 640)        \
+  X(203, reg, 4, 16, 16, 1024)       \
+  X(204, reg, 2, 32, 16, 1024)       \
+  X(205, reg, 2, 8, 8, 224)          \
+  X(206, reg, 3, 8, 8, 320)          \
+  X(207, reg, 4, 8, 8, 416)          \
+  X(208, reg, 1, 16, 16, 384)        \
+  X(209, reg, 1, 8, 8, 128)          \
+  X(210, reg, 2, 24, 24, 1024)       \
+  X(211, reg, 3, 22, 22, 1024)       \
+  X(212, reg, 4, 20, 20, 1024)       \
+  X(213, reg, 6, 8, 8, 704)          \
+  X(214, reg, 8, 8, 8, 1024)         \
+  X(215, reg, 6, 12, 12, 928)        \
+  X(216, reg, 5, 16, 16, 1024)       \
+  X(217, reg, 6, 14, 14, 1024)
 
 }  // namespace
 

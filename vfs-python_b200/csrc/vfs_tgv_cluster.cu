@@ -51,11 +51,19 @@ __device__ __forceinline__ float sget(const cg::cluster_group& cl, float* sm, in
   return remote[pl * kCMaxPx + (int)(g - (long)owner * b.stride)];
 }
 
+// Cluster-wide barrier; a cluster of one CTA needs only the CTA barrier,
+// which is much cheaper than the cluster barrier's arrive/wait round trip.
+__device__ __forceinline__ void csync(const cg::cluster_group& cl, bool single) {
+  if (single) __syncthreads();
+  else cl.sync();
+}
+
 __global__ void __launch_bounds__(kCNT, 1)
     k_tgv_cluster(TgvState st, TgvConsts cst, const float3* __restrict__ sched, int niter, SolverConsts kc,
                   Plane<float2> warp, Plane<float> ubefore, Plane<const float2> tvec, float limit, int h, int w,
                   int rows_per_cta) {
   cg::cluster_group cl = cg::this_cluster();
+  const bool single = cl.num_blocks() == 1;
   extern __shared__ float4 smem_raw[];
   float* const sm = reinterpret_cast<float*>(smem_raw);
   Band b;
@@ -105,7 +113,7 @@ __global__ void __launch_bounds__(kCNT, 1)
       sQW[e] = st.qw[f];
     }
   }
-  cl.sync();
+  csync(cl, single);
 
   for (int it = 0; it < niter; ++it) {
     const float3 ss = sched[it];  // (sigma, tau, mu)
@@ -140,7 +148,7 @@ __global__ void __launch_bounds__(kCNT, 1)
       sQZ[e] = q.z;
       sQW[e] = q.w;
     }
-    cl.sync();
+    csync(cl, single);
 #pragma unroll
     for (int j = 0; j < kCJ; ++j) {  // threshold + primal steps
       const int e = threadIdx.x + j * kCNT;
@@ -168,7 +176,7 @@ __global__ void __launch_bounds__(kCNT, 1)
       sVX[e] = vo.x;
       sVY[e] = vo.y;
     }
-    cl.sync();
+    csync(cl, single);
   }
 
   // ---- medianFilter + computeOpticalFlowWithClamp (Python/vfs.py:518-521)
@@ -177,7 +185,7 @@ __global__ void __launch_bounds__(kCNT, 1)
     const int e = threadIdx.x + j * kCNT;
     if (e < npx) sU[e] = ru[j];
   }
-  cl.sync();
+  csync(cl, single);
 #pragma unroll
   for (int j = 0; j < kCJ; ++j) {
     const int e = threadIdx.x + j * kCNT;
@@ -214,24 +222,18 @@ __global__ void __launch_bounds__(kCNT, 1)
     o.y = fmaf(delta, tv.y, o.y);
     warp.at(X, Y) = o;
   }
-  cl.sync();  // keep every CTA's shared memory alive until remote reads are done
+  csync(cl, single);  // keep every CTA's shared memory alive until remote reads are done
 }
 
 }  // namespace
 
 int tgv_cluster_size(int h, int w, int max_cluster) {
-  // smallest band count whose bands fit in a CTA, at most max_cluster; more
-  // CTAs spread small levels over more SMs
+  // the smallest band count whose bands fit in a CTA: every extra CTA adds
+  // cluster-barrier cost to each of the two phases of every iteration, and a
+  // level that fits one CTA runs with CTA barriers only
   if (h <= 0 || w <= 0 || w > kCMaxPx) return 0;
-  for (int cs = 1; cs <= max_cluster; cs *= 2) {
-    const int rows = (h + cs - 1) / cs;
-    if ((long)rows * w <= kCMaxPx) {
-      // prefer at least ~256 pixels per CTA while spreading the level
-      int best = cs;
-      while (best * 2 <= max_cluster && (long)((h + best * 2 - 1) / (best * 2)) * w >= 256) best *= 2;
-      return best;
-    }
-  }
+  for (int cs = 1; cs <= max_cluster; cs *= 2)
+    if ((long)((h + cs - 1) / cs) * w <= kCMaxPx) return cs;
   return 0;
 }
 
