@@ -238,6 +238,30 @@ VFS_API int vfs_plan_level_cluster(const VfsPlan* plan, int level);
 /* Select the fused TGV kernel variant by id (see vfs_tgv_variants). */
 VFS_API int vfs_plan_set_tgv_variant(VfsPlan* plan, int iters_per_launch);
 
+/* ---- Reverse mode (no counterpart in the reference, which is forward only).
+ * A gradient plan wraps a VfsPlan and differentiates
+ *   depth = triangulate_flow(solve_stereo(I_ref, I_other), t)[..., 2]
+ * with respect to both images, the translation t (which also moves the
+ * epipolar field get_vector_fields(grid, cam, cam, I, t, t_scale)) and
+ * theta = (Lambda, alpha0, alpha1, beta, gamma).  Images are float (h, w) in
+ * the u8 range (castAndScale divides by 256 inside).  vfs_grad_forward records
+ * a tape (flow, u, u_ at each warp's start and the solver state every
+ * `ckpt_every` iterations) in the workspace; vfs_grad_backward recomputes each
+ * checkpoint interval and runs the hand-written adjoint.  g_scalars receives
+ * 8 doubles on the device: dt0 dt1 dt2 dLambda dalpha0 dalpha1 dbeta dgamma.
+ * Set the mask on vfs_grad_plan(gp) before the first forward; per-level TGV
+ * variants set there are used by the forward (the cluster kernel is not). */
+typedef struct VfsGradPlan VfsGradPlan;
+VFS_API int vfs_grad_workspace_size(const VfsParams* prm, int ckpt_every, size_t* bytes);
+VFS_API int vfs_grad_create(const VfsParams* prm, int ckpt_every, float f, float u0, float v0, double t_scale,
+                            void* workspace, size_t workspace_bytes, VfsGradPlan** plan_out);
+VFS_API int vfs_grad_destroy(VfsGradPlan* plan);
+VFS_API VfsPlan* vfs_grad_plan(VfsGradPlan* plan);
+VFS_API int vfs_grad_forward(VfsGradPlan* plan, const float* img_ref, const float* img_other, const double* t,
+                             const double* theta, float* depth_out, void* stream);
+VFS_API int vfs_grad_backward(VfsGradPlan* plan, const float* g_depth, float* g_ref, float* g_other,
+                              double* g_scalars, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,7 +35,7 @@ def gold():
 
 # ---------------------------------------------------------------- C ABI, host side
 def test_library_exports_every_header_symbol(lib):
-    declared = re.findall(r"VFS_API\s+(?:int|size_t|const char\*)\s+(vfs_\w+)", open(HEADER).read())
+    declared = re.findall(r"VFS_API\s+(?:int|size_t|const char\*|VfsPlan\*)\s+(vfs_\w+)", open(HEADER).read())
     assert len(declared) >= 40
     out = subprocess.run(["nm", "-D", "--defined-only", lib.LIB_PATH], capture_output=True, text=True).stdout
     exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}

@@ -1,0 +1,132 @@
+"""GPU: the reverse mode of the solve (vfs_grad_*, DepthSolver) against the
+float64 reverse mode of oracle/np64/grad64.py on the same inputs."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import bench_params, pair
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(size=64, n_level=2, n_warp=3, n_iter=10, seed=0):
+    P = pair(size, t=(0.12, 0.01, 0.0), n_level=n_level, seed=seed)
+    prm = bench_params(size, size, n_level=n_level, n_warp=n_warp, n_iter=n_iter)
+    nz = np.random.default_rng(9)  # continuous images: no exact ties in the median windows
+    I0 = (P.img_ref + nz.uniform(0, 1, P.img_ref.shape)).astype(np.float32)
+    I1 = (P.img_other + nz.uniform(0, 1, P.img_other.shape)).astype(np.float32)
+    return P, prm, I0, I1
+
+
+def _solver(P, prm, ckpt=4):
+    from vfs_b200 import DepthSolver, EquidistantCam
+    return DepthSolver(prm, EquidistantCam(P.intrinsics), P.mask, t_scale=1.0, ckpt_every=ckpt)
+
+
+def _theta(prm):
+    return np.array([prm.Lambda, prm.alpha0, prm.alpha1, prm.beta, prm.gamma])
+
+
+def test_grad_forward_is_the_plain_solve():
+    """The recording forward gives the drop-in solve's depth bit for bit."""
+    from vfs_b200 import VFS, EquidistantCam
+    from vfs_b200.vector_field import get_vector_fields, get_grid_zero
+    P = pair(96, t=(0.12, 0.01, 0.0), n_level=3)
+    prm = bench_params(96, 96, n_level=3, n_warp=3, n_iter=20)
+    cam = EquidistantCam(P.intrinsics)
+    tvf, cvf = get_vector_fields(get_grid_zero(P.img_ref.shape), cam, cam, np.eye(3), P.t, 1)
+    v = VFS(prm)
+    v.setup_module()
+    v.compute_pyramid_sizes()
+    v.create_mask_pyramid(P.mask)
+    v.create_vector_field_pyramid(tvf, cvf)
+    v.solve_stereo(P.img_ref, P.img_other)
+    want = v.triangulate_flow(cam, P.t)[..., 2].cpu().numpy()
+    s = _solver(P, prm, ckpt=7)
+    got = s.forward_pass(torch.as_tensor(P.img_ref).float().cuda(), torch.as_tensor(P.img_other).float().cuda(),
+                         torch.tensor(P.t.reshape(3)), torch.tensor(_theta(prm))).cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def _gpu_grads(s, I0, I1, t, theta, wts):
+    d = s.forward_pass(torch.as_tensor(I0).cuda(), torch.as_tensor(I1).cuda(), torch.tensor(t), torch.tensor(theta))
+    g_ref, g_other, g_t, g_th = s.backward_pass(torch.as_tensor(wts, dtype=torch.float32).cuda())
+    torch.cuda.synchronize()
+    return d.cpu().numpy(), g_ref.cpu().numpy(), g_other.cpu().numpy(), g_t.cpu().numpy(), g_th.cpu().numpy()
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def test_grad_matches_float64_reverse_mode():
+    """Same inputs, same cotangent: CUDA float32 gradients against the float64
+    reverse mode run along the texture-quantised forward ("tex8")."""
+    from oracle.np64 import grad64 as G
+    from oracle.np64 import vfs64 as V
+    P, prm, I0, I1 = _problem()
+    t = P.t.reshape(3).astype(np.float64)
+    theta = _theta(prm)
+    s = _solver(P, prm, ckpt=4)
+    d, g_ref, g_other, g_t, g_th = _gpu_grads(s, I0, I1, t, theta, np.zeros(I0.shape))
+    good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
+    wts = np.where(good, np.random.default_rng(0).normal(0, 1, good.shape), 0.0)
+    d, g_ref, g_other, g_t, g_th = _gpu_grads(s, I0, I1, t, theta, wts)
+    prob = G.Problem(prm, V.EquidistantCam64(P.intrinsics), P.mask)
+    d64, tape = G.solve(prob, I0 / 256.0, I1 / 256.0, t, theta, mode="tex8", tape=True)
+    g = G.backward(prob, tape, wts)
+    # measured on a B200: 1.3e-4 (images), <= 2.5e-4 (scalars)
+    assert _rel(g_ref, g["I0"] / 256.0) < 2e-3
+    assert _rel(g_other, g["I1"] / 256.0) < 2e-3
+    for k in range(3):
+        assert abs(g_t[k] - g["t"][k]) <= 2e-3 * np.abs(g["t"]).max(), (k, g_t, g["t"])
+    for k in range(5):
+        assert abs(g_th[k] - g["theta"][k]) <= 2e-3 * abs(g["theta"][k]), (k, g_th, g["theta"])
+
+
+def test_grad_independent_of_checkpoint_spacing():
+    P, prm, I0, I1 = _problem(n_iter=9)
+    t = P.t.reshape(3).astype(np.float64)
+    theta = _theta(prm)
+    s = _solver(P, prm)
+    d = _gpu_grads(s, I0, I1, t, theta, np.zeros(I0.shape))[0]
+    s.release()
+    good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
+    wts = np.where(good, np.random.default_rng(1).normal(0, 1, good.shape), 0.0) * 1e-3
+    outs = []
+    for ck in (1, 4, 9, 100):
+        s = _solver(P, prm, ckpt=ck)
+        outs.append(_gpu_grads(s, I0, I1, t, theta, wts))
+        s.release()
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0])
+        for a, b in zip(o[1:], outs[0][1:]):
+            assert _rel(a, b) < 1e-4
+
+
+def test_autograd_function():
+    P, prm, I0, I1 = _problem(n_warp=2, n_iter=6)
+    s = _solver(P, prm, ckpt=3)
+    a = torch.as_tensor(I0).cuda().requires_grad_()
+    b = torch.as_tensor(I1).cuda().requires_grad_()
+    t = torch.tensor(P.t.reshape(3), dtype=torch.float64, requires_grad=True)
+    th = torch.tensor(_theta(prm), requires_grad=True)
+    depth = s(a, b, t, th)
+    m = torch.as_tensor(P.mask != 0).cuda() & torch.isfinite(depth) & (depth.abs() < 30)
+    gt = torch.as_tensor(P.depth).cuda()
+    loss = (depth - gt).abs()[m].mean()
+    depth2 = s(a, b, t, th)  # a second forward: the first one's backward records its tape again
+    loss.backward()
+    assert torch.isfinite(a.grad).all() and torch.isfinite(b.grad).all()
+    assert torch.isfinite(t.grad).all() and torch.isfinite(th.grad).all()
+    g_depth = torch.zeros_like(depth)
+    g_depth[m] = torch.sign((depth - gt)[m]) / m.sum()
+    s.forward_pass(a.detach(), b.detach(), t.detach(), th.detach())
+    g_ref, g_other, g_t, g_th = s.backward_pass(g_depth)
+    assert _rel(a.grad.cpu().numpy(), g_ref.cpu().numpy()) < 1e-5
+    assert _rel(th.grad.numpy(), g_th.cpu().numpy()) < 1e-5
+    assert torch.equal(depth2, depth)

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "vfs_b200", "libvfs_b200.so")
-SOURCES = ["vfs_capi.cu", "vfs_kernels.cu", "vfs_tgv.cu", "vfs_tgv_cluster.cu", "vfs_plan.cu", "vfs_batch.cu", "vfs_static.cu"]
+SOURCES = ["vfs_capi.cu", "vfs_kernels.cu", "vfs_tgv.cu", "vfs_tgv_cluster.cu", "vfs_plan.cu", "vfs_batch.cu", "vfs_static.cu", "vfs_grad.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -3,6 +3,7 @@
 // variants the solve path uses.  Launch shape: 32x8 threads, one pixel per
 // thread; these run once per level or once per warp, so they are a small
 // share of a solve next to the TGV iterations (vfs_tgv.cu).
+#include "vfs_camera.cuh"
 #include "vfs_kernels.cuh"
 #include "vfs_sample.cuh"
 
@@ -246,40 +247,6 @@ __global__ void k_mask_flow(Plane<float2> warp, Plane<const uint8_t> mask, int h
 __global__ void k_mask_code(Plane<uint8_t> code, Plane<const uint8_t> mask, int h, int w) {
   VFS_PIXEL_PROLOGUE
   code.at(X, Y) = mask_code(mask, X, Y, h, w);
-}
-
-// ---- camera (Python/equidistant_cam.cuh:32-59, Python/template_cam.cu:25-112)
-__device__ __forceinline__ float2 cam_project(const Cam& c, float3 X) {
-  const float R = hypotf(X.x, X.y);
-  const float theta = atan2f(R, X.z);
-  const float phi = atan2f(X.y, X.x);
-  float2 uv;
-  sincosf(phi, &(uv.y), &(uv.x));
-  uv.x = fmaf(c.f * theta, uv.x, c.u0);
-  uv.y = fmaf(c.f * theta, uv.y, c.v0);
-  return uv;
-}
-
-__device__ __forceinline__ float3 cam_unproject(const Cam& c, float2 x) {
-  const float2 xy = make_float2(x.x - c.u0, x.y - c.v0);
-  const float theta = hypotf(xy.x, xy.y) / c.f;
-  const float phi = atan2f(xy.y, xy.x);
-  float3 X;
-  sincosf(phi, &(X.y), &(X.x));
-  float2 sc;
-  sincosf(theta, &(sc.x), &(sc.y));
-  X.x *= sc.x;
-  X.y *= sc.x;
-  X.z = sc.y;
-  return X;
-}
-
-// triangulateRays, Python/vfs.cu:707-735.
-__device__ __forceinline__ float3 triangulate_px(float3 rr, float3 ro, float tx, float tz) {
-  const float2 xyRef = make_float2(rr.x / rr.z, rr.y / rr.z);
-  const float2 xyOther = make_float2(ro.x / ro.z, ro.y / ro.z);
-  const float ZRef = fmaf(-tz, xyOther.x, tx) / fmaf(-1, xyRef.x, xyOther.x);
-  return make_float3(ZRef * xyRef.x, ZRef * xyRef.y, ZRef);
 }
 
 __global__ void k_triangulate(float3* out, const float3* __restrict__ rays, const float3* __restrict__ rays_o,

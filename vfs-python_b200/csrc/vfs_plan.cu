@@ -77,6 +77,22 @@ __global__ void k_derivs_init(TgvConsts out, TgvState st, Plane<const float> ube
 }
 
 }  // namespace
+
+cudaError_t launch_tensor_soa(const TgvConsts& out, uint8_t* code, cudaTextureObject_t smooth,
+                              Plane<const uint8_t> mask, const SolverConsts& k, int h, int w, cudaStream_t s) {
+  if (h <= 0 || w <= 0) return cudaSuccess;
+  k_tensor_soa<<<grid2d(h, w), dim3(kBX, kBY), 0, s>>>(out, code, smooth, mask, k, h, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_derivs_init(const TgvConsts& out, const TgvState& st, Plane<const float> ubefore,
+                               Plane<const float> ub_src, cudaTextureObject_t tref, cudaTextureObject_t twarped,
+                               cudaTextureObject_t tdir, int h, int w, cudaStream_t s) {
+  if (h <= 0 || w <= 0) return cudaSuccess;
+  k_derivs_init<<<grid2d(h, w), dim3(kBX, kBY), 0, s>>>(out, st, ubefore, ub_src, tref, twarped, tdir, h, w);
+  return cudaGetLastError();
+}
+
 }  // namespace vfs
 
 using namespace vfs;

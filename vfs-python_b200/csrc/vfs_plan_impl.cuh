@@ -86,4 +86,13 @@ int plan_warp_post(VfsPlan* pl, LevelCtx* c, cudaStream_t s, long long* nk);
 int plan_level_end(VfsPlan* pl, LevelCtx* c, cudaStream_t s, long long* nk);
 int plan_finish(VfsPlan* pl, cudaStream_t s, long long* nk);
 
+// computeTensorEtaMasked into the solver's constant planes plus the mask
+// code (Python/vfs.cu:239-281), and computeDerivatives plus the per-warp
+// solver reset (Python/vfs.cu:304-324, Python/vfs.py:486-497).
+cudaError_t launch_tensor_soa(const TgvConsts& out, uint8_t* code, cudaTextureObject_t smooth,
+                              Plane<const uint8_t> mask, const SolverConsts& k, int h, int w, cudaStream_t s);
+cudaError_t launch_derivs_init(const TgvConsts& out, const TgvState& st, Plane<const float> ubefore,
+                               Plane<const float> ub_src, cudaTextureObject_t tref, cudaTextureObject_t twarped,
+                               cudaTextureObject_t tdir, int h, int w, cudaStream_t s);
+
 }  // namespace vfs

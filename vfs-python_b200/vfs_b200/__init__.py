@@ -11,6 +11,7 @@ from .vfs import VFS
 from .equidistant_cam import EquidistantCam
 from .vector_field import get_vector_fields, get_grid_zero, get_grid_one, default_normalizer
 from .texture import create_texture_object
+from .grad import DepthSolver
 
 __all__ = ["VFS", "vfs_params", "EquidistantCam", "get_vector_fields", "get_grid_zero", "get_grid_one",
-           "default_normalizer", "create_texture_object"]
+           "default_normalizer", "create_texture_object", "DepthSolver"]

@@ -114,6 +114,12 @@ _SIGS = {
     "vfs_plan_level_cluster": [_P, _I],
     "vfs_plan_stats": [_P, ctypes.POINTER(VfsSolveStats)],
     "vfs_step_schedule": [_I, _D, _P],
+    "vfs_grad_workspace_size": [_PRM, _I, ctypes.POINTER(_SZ)],
+    "vfs_grad_create": [_PRM, _I, _F, _F, _F, _D, _P, _SZ, ctypes.POINTER(_P)],
+    "vfs_grad_destroy": [_P],
+    "vfs_grad_plan": [_P],
+    "vfs_grad_forward": [_P, _P, _P, _P, _P, _P, _P],
+    "vfs_grad_backward": [_P, _P, _P, _P, _P, _P],
 }
 
 _lib = None
@@ -131,7 +137,8 @@ def lib() -> ctypes.CDLL:
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = (ctypes.c_char_p if name == "vfs_last_error" else
-                          ctypes.c_size_t if name == "vfs_static_scratch_bytes" else ctypes.c_int)
+                          ctypes.c_size_t if name == "vfs_static_scratch_bytes" else
+                          ctypes.c_void_p if name == "vfs_grad_plan" else ctypes.c_int)
         _lib = L
     return _lib
 

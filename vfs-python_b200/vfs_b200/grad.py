@@ -1,0 +1,133 @@
+"""Differentiable depth from the stereo solve (no counterpart in the reference,
+which is forward only).
+
+``DepthSolver`` fixes what is not differentiated (the parameter bag's loop
+counts, fScale, limitRange and timeStepLambda, the camera, the mask,
+``t_scale``) and maps
+
+    (img_ref, img_other, t, theta) -> depth = triangulate_flow(solve_stereo(...), t)[..., 2]
+
+with theta = (Lambda, alpha0, alpha1, beta, gamma).  The translation also
+moves the epipolar field, ``get_vector_fields(grid, cam, cam, I, t, t_scale)``.
+Images are float32 CUDA tensors in the u8 range (u8 images converted with
+``.float()`` give the plain solve's result bit for bit).  The backward pass is
+the hand-written reverse mode of libvfs_b200 (``vfs_grad_*``): the forward
+records the flow, u and u_ at each warp's start and the solver state every
+``ckpt_every`` iterations; the backward recomputes each interval and runs the
+adjoint kernels.
+
+    solver = DepthSolver(param, camera, mask)
+    depth = solver(img_ref, img_other, t, theta)       # autograd-aware
+    loss = (depth - gt).abs()[mask != 0].mean(); loss.backward()
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr, stream
+
+THETA = ("Lambda", "alpha0", "alpha1", "beta", "gamma")
+
+
+class DepthSolver:
+    def __init__(self, param, camera, mask, t_scale: float = 1.0, ckpt_every: int = 10, level_variants=None):
+        self.param = param
+        self.prm = _lib.VfsParams.from_param_bag(param)
+        self.ckpt_every = int(ckpt_every)
+        need = ctypes.c_size_t(0)
+        call("vfs_grad_workspace_size", ctypes.byref(self.prm), self.ckpt_every, ctypes.byref(need))
+        self.workspace_bytes = int(need.value)
+        self._ws = torch.empty(self.workspace_bytes + 1024, dtype=torch.uint8, device="cuda")
+        gp = ctypes.c_void_p(0)
+        f, u0, v0 = camera._k() if hasattr(camera, "_k") else (float(x) for x in camera)
+        call("vfs_grad_create", ctypes.byref(self.prm), self.ckpt_every, f, u0, v0, float(t_scale),
+             self._ws.data_ptr(), self._ws.numel(), ctypes.byref(gp))
+        self._gp = gp
+        self.shape = (int(param.height), int(param.width))
+        m = mask if isinstance(mask, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(mask))
+        self._mask = m.to(device="cuda", dtype=torch.uint8).contiguous()
+        if tuple(self._mask.shape) != self.shape:
+            raise AssertionError(f"mask shape {tuple(self._mask.shape)} != {self.shape}")
+        self._plan = _lib.lib().vfs_grad_plan(self._gp)
+        call("vfs_plan_set_mask", self._plan, self._mask.data_ptr(), self.shape[1], stream())
+        for lvl, var in enumerate(level_variants or []):
+            if var:
+                call("vfs_plan_set_level_variant", self._plan, lvl, int(var))
+        self._scal = torch.zeros(8, dtype=torch.float64, device="cuda")
+        self._generation = 0
+        self._recorded = None
+
+    def theta_of(self, param=None) -> torch.Tensor:
+        p = param or self.param
+        return torch.tensor([float(getattr(p, k)) for k in THETA], dtype=torch.float64)
+
+    def __call__(self, img_ref, img_other, t, theta=None):
+        if theta is None:
+            theta = self.theta_of()
+        return _DepthFunction.apply(self, img_ref, img_other, torch.as_tensor(t, dtype=torch.float64),
+                                    torch.as_tensor(theta, dtype=torch.float64))
+
+    # ---- the two passes (also usable without autograd)
+    def _check(self, img, what):
+        _lib.require_cuda(img, what)
+        if img.dtype != torch.float32 or tuple(img.shape) != self.shape:
+            raise AssertionError(f"{what} must be float32 {self.shape}")
+
+    def forward_pass(self, img_ref, img_other, t, theta) -> torch.Tensor:
+        self._check(img_ref, "img_ref")
+        self._check(img_other, "img_other")
+        tv = [float(x) for x in torch.as_tensor(t, dtype=torch.float64).reshape(3).tolist()]
+        th = [float(x) for x in torch.as_tensor(theta, dtype=torch.float64).reshape(5).tolist()]
+        depth = torch.empty(self.shape, dtype=torch.float32, device="cuda")
+        call("vfs_grad_forward", self._gp, img_ref.data_ptr(), img_other.data_ptr(), (ctypes.c_double * 3)(*tv),
+             (ctypes.c_double * 5)(*th), depth.data_ptr(), stream())
+        self._generation += 1
+        return depth
+
+    def backward_pass(self, g_depth: torch.Tensor):
+        g_depth = g_depth.to(device="cuda", dtype=torch.float32).contiguous()
+        g_ref = torch.empty(self.shape, dtype=torch.float32, device="cuda")
+        g_other = torch.empty(self.shape, dtype=torch.float32, device="cuda")
+        call("vfs_grad_backward", self._gp, g_depth.data_ptr(), g_ref.data_ptr(), g_other.data_ptr(),
+             self._scal.data_ptr(), stream())
+        return g_ref, g_other, self._scal[:3].clone(), self._scal[3:].clone()
+
+    def release(self) -> None:
+        if self._gp:
+            torch.cuda.current_stream().synchronize()
+            _lib.lib().vfs_grad_destroy(self._gp)
+            self._gp = None
+            self._ws = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class _DepthFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, solver, img_ref, img_other, t, theta):
+        depth = solver.forward_pass(img_ref.detach(), img_other.detach(), t.detach(), theta.detach())
+        ctx.solver = solver
+        ctx.generation = solver._generation
+        ctx.save_for_backward(img_ref, img_other, t, theta)
+        return depth
+
+    @staticmethod
+    def backward(ctx, g_depth):
+        solver = ctx.solver
+        img_ref, img_other, t, theta = ctx.saved_tensors
+        if solver._generation != ctx.generation:
+            # another forward ran on this solver since: record this one's tape again
+            solver.forward_pass(img_ref.detach(), img_other.detach(), t.detach(), theta.detach())
+            ctx.generation = solver._generation
+        g_ref, g_other, g_t, g_theta = solver.backward_pass(g_depth)
+        return (None, g_ref if ctx.needs_input_grad[1] else None, g_other if ctx.needs_input_grad[2] else None,
+                g_t.to(t.device) if ctx.needs_input_grad[3] else None,
+                g_theta.to(theta.device) if ctx.needs_input_grad[4] else None)
