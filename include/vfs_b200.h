@@ -261,6 +261,12 @@ VFS_API int vfs_grad_forward(VfsGradPlan* plan, const float* img_ref, const floa
                              const double* theta, float* depth_out, void* stream);
 VFS_API int vfs_grad_backward(VfsGradPlan* plan, const float* g_depth, float* g_ref, float* g_other,
                               double* g_scalars, void* stream);
+/* Backward kernels: fused_reverse 1..5 reverses an iteration in one tiled
+ * kernel of that tile shape (1, the default: 32x16; 2: 32x8; 3: 64x8;
+ * 4: 32x32; 5: 28x16), 0 in three gather kernels; trace_variant selects the TGV
+ * variant that recomputes checkpoint intervals (0: automatic, -1: one
+ * iteration per launch). */
+VFS_API int vfs_grad_set_options(VfsGradPlan* plan, int fused_reverse, int trace_variant);
 
 #ifdef __cplusplus
 }

@@ -130,3 +130,22 @@ def test_autograd_function():
     assert _rel(a.grad.cpu().numpy(), g_ref.cpu().numpy()) < 1e-5
     assert _rel(th.grad.numpy(), g_th.cpu().numpy()) < 1e-5
     assert torch.equal(depth2, depth)
+
+
+def test_backward_kernel_forms_agree():
+    """Tiled and three-kernel reverse steps, recording and one-iteration
+    recomputation: the same gradients (float atomics reorder sums only)."""
+    P, prm, I0, I1 = _problem(n_iter=9)
+    t = P.t.reshape(3).astype(np.float64)
+    theta = _theta(prm)
+    s = _solver(P, prm, ckpt=5)
+    d = _gpu_grads(s, I0, I1, t, theta, np.zeros(I0.shape))[0]
+    good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
+    wts = np.where(good, np.random.default_rng(2).normal(0, 1, good.shape), 0.0) * 1e-3
+    outs = []
+    for fused, tv in ((0, -1), (1, -1), (0, 0), (1, 0), (1, 124), (1, 216), (2, 0), (3, 0), (4, 0), (5, 0)):
+        s.set_options(fused, tv)
+        outs.append(_gpu_grads(s, I0, I1, t, theta, wts))
+    for o in outs[1:]:
+        for a, b in zip(o[1:], outs[0][1:]):
+            assert _rel(a, b) < 1e-5

@@ -62,11 +62,11 @@ __device__ __forceinline__ T ld0(const T* a, long i, long n) {
   return (i >= 0 && i < n) ? a[i] : T(0);
 }
 
-// Sum of N per-thread values over the (256-thread) block, added to out[0..N).
-// Every thread of the block must call it.
+// Sum of N per-thread values over the block (at most 1024 threads), added to
+// out[0..N).  Every thread of the block must call it.
 template <int N>
 __device__ __forceinline__ void block_sum_to(const float (&v)[N], double* out) {
-  __shared__ float red[N][kGX * kGY / 32];
+  __shared__ float red[N][32];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int lane = tid & 31, wid = tid >> 5;
 #pragma unroll
@@ -529,6 +529,398 @@ __global__ void __launch_bounds__(kGX* kGY) k_rev3(RevArgs r) {
   r.g0.vby[i] = gvy;
 }
 
+// The three phases above in one kernel over a TX x TY tile.  The window is
+// the tile plus 2 pixels on every side in flat addressing (window pixel
+// (wx, wy) is flat index (y0-2+wy)*w + (x0-2+wx), so window neighbours are the
+// flat neighbours, row wrap included).  Phase 1 runs on the window minus its
+// first row and column, phase 2 on the tile plus 1 pixel, phase 3 on the
+// tile; the values passed between phases stay in shared memory.
+enum RevPlane { qUB, qVX, qVY, qPX, qPY, qQX, qQY, qQZ, qQW, qA, qB, qC, aX, aY, aB, c0, c1, c2, c3, c4, c5, lUB, lVX,
+                lVY, kRevPlanes };
+
+template <int TX, int TY>
+struct RevGeom {
+  static constexpr int WX = TX + 4, WY = TY + 4, N = WX * WY;
+  static constexpr size_t smem_bytes() { return (size_t)kRevPlanes * N * sizeof(float) + ((N + 15) / 16) * 16; }
+};
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_rev_tile(RevArgs r) {
+  using G = RevGeom<TX, TY>;
+  constexpr int WX = G::WX, WY = G::WY, N = G::N;
+  extern __shared__ float4 smem_raw[];
+  float* const sm = reinterpret_cast<float*>(smem_raw);
+  uint8_t* const scode = reinterpret_cast<uint8_t*>(sm + (size_t)kRevPlanes * N);
+  auto P = [&](int plane) { return sm + (size_t)plane * N; };
+  const int w = r.w, h = r.h;
+  const long n = (long)h * w;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const long base = (long)(y0 - 2) * w + (x0 - 2);
+  const float eps = 1E-7f;
+  const float mu = r.mu, tau = r.tau, sigma = r.sigma, al0 = r.k.alpha0, al1 = r.k.alpha1, lam = r.k.lambda;
+  const float* __restrict__ const S0U = r.s0.u;
+  const float* __restrict__ const S0UB = r.s0.ub;
+  const float* __restrict__ const S0VX = r.s0.vbx;
+  const float* __restrict__ const S0VY = r.s0.vby;
+  const float* __restrict__ const S0PX = r.s0.px;
+  const float* __restrict__ const S0PY = r.s0.py;
+  const float* __restrict__ const S0QX = r.s0.qx;
+  const float* __restrict__ const S0QY = r.s0.qy;
+  const float* __restrict__ const S0QZ = r.s0.qz;
+  const float* __restrict__ const S0QW = r.s0.qw;
+  const float* __restrict__ const S1U = r.s1.u;
+  const float* __restrict__ const S1UB = r.s1.ub;
+  const float* __restrict__ const S1VX = r.s1.vbx;
+  const float* __restrict__ const S1VY = r.s1.vby;
+  const float* __restrict__ const S1PX = r.s1.px;
+  const float* __restrict__ const S1PY = r.s1.py;
+  const float* __restrict__ const S1QX = r.s1.qx;
+  const float* __restrict__ const S1QY = r.s1.qy;
+  const float* __restrict__ const S1QZ = r.s1.qz;
+  const float* __restrict__ const S1QW = r.s1.qw;
+  const float* __restrict__ const G1U = r.g1.u;
+  const float* __restrict__ const G1UB = r.g1.ub;
+  const float* __restrict__ const G1VX = r.g1.vbx;
+  const float* __restrict__ const G1VY = r.g1.vby;
+  const float* __restrict__ const G1PX = r.g1.px;
+  const float* __restrict__ const G1PY = r.g1.py;
+  const float* __restrict__ const G1QX = r.g1.qx;
+  const float* __restrict__ const G1QY = r.g1.qy;
+  const float* __restrict__ const G1QZ = r.g1.qz;
+  const float* __restrict__ const G1QW = r.g1.qw;
+  float* __restrict__ const G0U = r.g0.u;
+  float* __restrict__ const G0UB = r.g0.ub;
+  float* __restrict__ const G0VX = r.g0.vbx;
+  float* __restrict__ const G0VY = r.g0.vby;
+  float* __restrict__ const G0PX = r.g0.px;
+  float* __restrict__ const G0PY = r.g0.py;
+  float* __restrict__ const G0QX = r.g0.qx;
+  float* __restrict__ const G0QY = r.g0.qy;
+  float* __restrict__ const G0QZ = r.g0.qz;
+  float* __restrict__ const G0QW = r.g0.qw;
+  const float* __restrict__ const CA = r.c.a;
+  const float* __restrict__ const CB = r.c.b;
+  const float* __restrict__ const CC = r.c.c;
+  const float* __restrict__ const CEX = r.c.ex;
+  const float* __restrict__ const CEY = r.c.ey;
+  const float* __restrict__ const CEZ = r.c.ez;
+  const float* __restrict__ const CIU = r.c.iu;
+  const float* __restrict__ const CIZ = r.c.iz;
+  const uint8_t* __restrict__ const CCODE = r.c.code;
+  float* __restrict__ const GC0 = r.gc[0];
+  float* __restrict__ const GC1 = r.gc[1];
+  float* __restrict__ const GC2 = r.gc[2];
+  float* __restrict__ const GC3 = r.gc[3];
+  float* __restrict__ const GC4 = r.gc[4];
+  float* __restrict__ const GC5 = r.gc[5];
+  float* __restrict__ const GC6 = r.gc[6];
+  float* __restrict__ const GC7 = r.gc[7];
+  float acc[3] = {0.f, 0.f, 0.f};  // Lambda, alpha0, alpha1
+
+#pragma unroll
+  for (int j = 0; j < (N + NT - 1) / NT; ++j) {
+    const int e = threadIdx.x + j * NT;
+    if (e >= N) continue;
+    const int wy = e / WX, wx = e - wy * WX;
+    const long f = base + (long)wy * w + wx;
+    const bool ok = f >= 0 && f < n;
+    P(qUB)[e] = ok ? S0UB[f] : 0.f;
+    P(qVX)[e] = ok ? S0VX[f] : 0.f;
+    P(qVY)[e] = ok ? S0VY[f] : 0.f;
+    P(qPX)[e] = ok ? S1PX[f] : 0.f;
+    P(qPY)[e] = ok ? S1PY[f] : 0.f;
+    P(qQX)[e] = ok ? S1QX[f] : 0.f;
+    P(qQY)[e] = ok ? S1QY[f] : 0.f;
+    P(qQZ)[e] = ok ? S1QZ[f] : 0.f;
+    P(qQW)[e] = ok ? S1QW[f] : 0.f;
+    P(qA)[e] = ok ? CA[f] : 0.f;
+    P(qB)[e] = ok ? CB[f] : 0.f;
+    P(qC)[e] = ok ? CC[f] : 0.f;
+    scode[e] = ok ? CCODE[f] : 0;
+  }
+  __syncthreads();
+
+  // phase 1: primal and threshold reversed, on [1, WX) x [1, WY)
+#pragma unroll
+  for (int j = 0; j < (N + NT - 1) / NT; ++j) {
+    const int e = threadIdx.x + j * NT;
+    if (e >= N) continue;
+    const int wy = e / WX, wx = e - wy * WX;
+    if (wx < 1 || wy < 1) continue;
+    const long f = base + (long)wy * w + wx;
+    const uint8_t c = scode[e];
+    const bool core = wx >= 2 && wx < TX + 2 && wy >= 2 && wy < TY + 2 && x0 + wx - 2 < w && y0 + wy - 2 < h;
+    float gu = 0.f, gubl = 0.f, gvx = 0.f, gvy = 0.f, Ax = 0.f, Ay = 0.f, Bv = 0.f;
+    if (f >= 0 && f < n && (c & kSelf)) {
+      const float gubn = G1UB[f];
+      const float gvbx = G1VX[f], gvby = G1VY[f];
+      const float gun = G1U[f] + (1.f + mu) * gubn;
+      const float gVx = (1.f + mu) * gvbx, gVy = (1.f + mu) * gvby;
+      const float a = P(qA)[e], b = P(qB)[e], cc = P(qC)[e];
+      const float gQx = ((c & kE) ? P(qQX)[e] : 0.f) - ((c & kW) ? P(qQX)[e - 1] : 0.f);
+      const float gQw = ((c & kE) ? P(qQW)[e] : 0.f) - ((c & kW) ? P(qQW)[e - 1] : 0.f);
+      const float gQy = ((c & kS) ? P(qQY)[e] : 0.f) - ((c & kN) ? P(qQY)[e - WX] : 0.f);
+      const float gQz = ((c & kS) ? P(qQZ)[e] : 0.f) - ((c & kN) ? P(qQZ)[e - WX] : 0.f);
+      const float px = P(qPX)[e], py = P(qPY)[e];
+      const float tpx = fmaf(a, px, cc * py), tpy = fmaf(cc, px, b * py);
+      const float ex = CEX[f], ey = CEY[f], ez = CEZ[f];
+      const bool sx = fabsf(ex) < eps, sy = fabsf(ey) < eps, sz = fabsf(ez) < eps;
+      const float t1 = sy ? tau : tau / ey, t2 = sz ? tau : tau / ez;
+      Ax = t1 * al0 * gVx;
+      Ay = t2 * al0 * gVy;
+      const float tpWx = fmaf(P(qA)[e - 1], P(qPX)[e - 1], P(qC)[e - 1] * P(qPY)[e - 1]);
+      const float tpNy = fmaf(P(qC)[e - WX], P(qPX)[e - WX], P(qB)[e - WX] * P(qPY)[e - WX]);
+      const bool E_ = c & kE, W_ = c & kW, S_ = c & kS, N_ = c & kN;
+      const float gTx = (E_ && W_) ? tpx - tpWx : (!E_ ? -tpWx : tpx);
+      const float gTy = (S_ && N_) ? tpy - tpNy : (!S_ ? -tpNy : tpy);
+      const float Iu = CIU[f], Iz = CIZ[f];
+      const float te = sx ? tau : tau / ex;
+      const float u = S0U[f], ub = P(qUB)[e];
+      const float ut = ub + te * (gTx + gTy);
+      const float rho = Iu * (ut - u) + Iz;
+      const float Bd = lam * te * Iu * Iu;
+      float gut = 0.f, gte = 0.f, giu = 0.f, giz = 0.f, gl = 0.f;
+      if ((rho <= Bd) && (rho >= -Bd)) {
+        if (fabsf(Iu) >= eps) {
+          gu += gun;
+          giz = -gun / Iu;
+          giu = gun * Iz / (Iu * Iu);
+        } else {
+          gut = gun;
+        }
+      } else if (rho < -Bd) {
+        gut = gun;
+        gl = te * Iu * gun;
+        gte = lam * Iu * gun;
+        giu = lam * te * gun;
+      } else if (rho > Bd) {
+        gut = gun;
+        gl = -te * Iu * gun;
+        gte = -lam * Iu * gun;
+        giu = -lam * te * gun;
+      } else {
+        gu += gun;
+      }
+      gte += (gTx + gTy) * gut;
+      Bv = te * gut;
+      gubl = -mu * gubn + gut;
+      gvx = gVx - mu * gvbx;
+      gvy = gVy - mu * gvby;
+      if (core) {
+        const float inx = fmaf(al1, tpx, al0 * (gQx + gQz));
+        const float iny = fmaf(al1, tpy, al0 * (gQw + gQy));
+        GC3[f] += sx ? 0.f : -te / ex * gte;
+        GC4[f] += sy ? 0.f : -t1 / ey * inx * gVx;
+        GC5[f] += sz ? 0.f : -t2 / ez * iny * gVy;
+        GC6[f] += giu;
+        GC7[f] += giz;
+        acc[0] += gl;
+        acc[1] += t1 * (gQx + gQz) * gVx + t2 * (gQw + gQy) * gVy;
+        acc[2] += t1 * tpx * gVx + t2 * tpy * gVy;
+      }
+    }
+    P(aX)[e] = Ax;
+    P(aY)[e] = Ay;
+    P(aB)[e] = Bv;
+    if (core) {
+      G0U[f] = gu;
+      P(lUB)[e] = gubl;
+      P(lVX)[e] = gvx;
+      P(lVY)[e] = gvy;
+    }
+  }
+  __syncthreads();
+
+  // phase 2: dual step reversed, on [1, WX - 1) x [1, WY - 1)
+#pragma unroll
+  for (int j = 0; j < (N + NT - 1) / NT; ++j) {
+    const int e = threadIdx.x + j * NT;
+    if (e >= N) continue;
+    const int wy = e / WX, wx = e - wy * WX;
+    if (wx < 1 || wy < 1 || wx >= WX - 1 || wy >= WY - 1) continue;
+    const long f = base + (long)wy * w + wx;
+    const uint8_t c = scode[e];
+    const bool core = wx >= 2 && wx < TX + 2 && wy >= 2 && wy < TY + 2 && x0 + wx - 2 < w && y0 + wy - 2 < h;
+    float Cv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (f >= 0 && f < n && (c & kSelf)) {
+      const uint8_t cE = scode[e + 1], cS = scode[e + WX];
+      const float Bv = P(aB)[e];
+      const float gVx = (1.f + mu) * G1VX[f], gVy = (1.f + mu) * G1VY[f];
+      const float ey = CEY[f], ez = CEZ[f];
+      const float t1 = fabsf(ey) < eps ? tau : tau / ey, t2 = fabsf(ez) < eps ? tau : tau / ez;
+      const float gtpx = t1 * al1 * gVx + ((c & kE) ? Bv : 0.f) - (((cE & kW) || !(cE & kE)) ? P(aB)[e + 1] : 0.f);
+      const float gtpy = t2 * al1 * gVy + ((c & kS) ? Bv : 0.f) - (((cS & kN) || !(cS & kS)) ? P(aB)[e + WX] : 0.f);
+      const float Ax = P(aX)[e], Ay = P(aY)[e];
+      float gq0 = G1QX[f] + ((c & kE) ? Ax : 0.f) - ((cE & kW) ? P(aX)[e + 1] : 0.f);
+      float gq3 = G1QW[f] + ((c & kE) ? Ay : 0.f) - ((cE & kW) ? P(aY)[e + 1] : 0.f);
+      float gq1 = G1QY[f] + ((c & kS) ? Ay : 0.f) - ((cS & kN) ? P(aY)[e + WX] : 0.f);
+      float gq2 = G1QZ[f] + ((c & kS) ? Ax : 0.f) - ((cS & kN) ? P(aX)[e + WX] : 0.f);
+      const float a = P(qA)[e], b = P(qB)[e], cc = P(qC)[e];
+      const float pnx = P(qPX)[e], pny = P(qPY)[e];
+      const float gpx = G1PX[f] + fmaf(a, gtpx, cc * gtpy);
+      const float gpy = G1PY[f] + fmaf(cc, gtpx, b * gtpy);
+      float ga = pnx * gtpx, gb = pny * gtpy, gcc = pny * gtpx + pnx * gtpy;
+      const float uc = P(qUB)[e], vcx = P(qVX)[e], vcy = P(qVY)[e];
+      float gUx, gUy, gVxx, gVyy, gVz, gVw;
+      if (c & kE) {
+        gUx = P(qUB)[e + 1] - uc - vcx;
+        gVxx = P(qVX)[e + 1] - vcx;
+        gVw = P(qVY)[e + 1] - vcy;
+      } else {
+        gUx = uc - P(qUB)[e - 1] - vcx;
+        gVxx = vcx - P(qVX)[e - 1];
+        gVw = vcy - P(qVY)[e - 1];
+      }
+      if (c & kS) {
+        gUy = P(qUB)[e + WX] - uc - vcy;
+        gVyy = P(qVY)[e + WX] - vcy;
+        gVz = P(qVX)[e + WX] - vcx;
+      } else {
+        gUy = uc - P(qUB)[e - WX] - vcy;
+        gVyy = vcy - P(qVY)[e - WX];
+        gVz = vcx - P(qVX)[e - WX];
+      }
+      const float scaleP = al1 * sigma / r.k.etaP;
+      const float scaleQ = al0 * sigma / r.k.etaQ;
+      const float tux = fmaf(a, gUx, cc * gUy), tuy = fmaf(cc, gUx, b * gUy);
+      const float upx = fmaf(scaleP, tux, S0PX[f]), upy = fmaf(scaleP, tuy, S0PY[f]);
+      const float nP = hypotf(upx, upy);
+      float gP0 = gpx, gP1 = gpy;
+      if (nP > 1.f) {
+        const float dt = pnx * gpx + pny * gpy;
+        gP0 = (gpx - pnx * dt) / nP;
+        gP1 = (gpy - pny * dt) / nP;
+      }
+      const float uq0 = fmaf(scaleQ, gVxx, S0QX[f]), uq1 = fmaf(scaleQ, gVyy, S0QY[f]);
+      const float uq2 = fmaf(scaleQ, gVz, S0QZ[f]), uq3 = fmaf(scaleQ, gVw, S0QW[f]);
+      const float nQ = norm4df(uq0, uq1, uq2, uq3);
+      if (nQ > 1.f) {
+        const float q0 = P(qQX)[e], q1 = P(qQY)[e], q2 = P(qQZ)[e], q3 = P(qQW)[e];
+        const float dt = q0 * gq0 + q1 * gq1 + q2 * gq2 + q3 * gq3;
+        gq0 = (gq0 - q0 * dt) / nQ;
+        gq1 = (gq1 - q1 * dt) / nQ;
+        gq2 = (gq2 - q2 * dt) / nQ;
+        gq3 = (gq3 - q3 * dt) / nQ;
+      }
+      const float gtux = scaleP * gP0, gtuy = scaleP * gP1;
+      Cv[0] = fmaf(a, gtux, cc * gtuy);
+      Cv[1] = fmaf(cc, gtux, b * gtuy);
+      Cv[2] = scaleQ * gq0;
+      Cv[3] = scaleQ * gq1;
+      Cv[4] = scaleQ * gq2;
+      Cv[5] = scaleQ * gq3;
+      if (core) {
+        ga += gUx * gtux;
+        gb += gUy * gtuy;
+        gcc += gUy * gtux + gUx * gtuy;
+        GC0[f] += ga;
+        GC1[f] += gb;
+        GC2[f] += gcc;
+        acc[1] += sigma / r.k.etaQ * (gVxx * gq0 + gVyy * gq1 + gVz * gq2 + gVw * gq3);
+        acc[2] += sigma / r.k.etaP * (tux * gP0 + tuy * gP1);
+        G0PX[f] = gP0;
+        G0PY[f] = gP1;
+        G0QX[f] = gq0;
+        G0QY[f] = gq1;
+        G0QZ[f] = gq2;
+        G0QW[f] = gq3;
+      }
+    } else if (core) {
+      G0PX[f] = G0PY[f] = 0.f;
+      G0QX[f] = G0QY[f] = G0QZ[f] = G0QW[f] = 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) P(c0 + k)[e] = Cv[k];
+  }
+  __syncthreads();
+
+  // phase 3: transposed gradients of u_ and v_, on the tile
+#pragma unroll
+  for (int j = 0; j < (N + NT - 1) / NT; ++j) {
+    const int e = threadIdx.x + j * NT;
+    if (e >= N) continue;
+    const int wy = e / WX, wx = e - wy * WX;
+    if (wx < 2 || wy < 2 || wx >= TX + 2 || wy >= TY + 2 || x0 + wx - 2 >= w || y0 + wy - 2 >= h) continue;
+    const long f = base + (long)wy * w + wx;
+    const uint8_t c = scode[e];
+    float gub = P(lUB)[e], gvx = P(lVX)[e], gvy = P(lVY)[e];
+    if (c & kSelf) {
+      const float u0 = P(c0)[e], u1 = P(c1)[e];
+      const float v0 = P(c2)[e], v1 = P(c3)[e], v2 = P(c4)[e], v3 = P(c5)[e];
+      gub += ((c & kE) ? -u0 : u0) + ((c & kS) ? -u1 : u1);
+      gvx += -u0 + ((c & kE) ? -v0 : v0) + ((c & kS) ? -v2 : v2);
+      gvy += -u1 + ((c & kE) ? -v3 : v3) + ((c & kS) ? -v1 : v1);
+    }
+    if (scode[e - 1] & kE) {
+      gub += P(c0)[e - 1];
+      gvx += P(c2)[e - 1];
+      gvy += P(c5)[e - 1];
+    }
+    if (!(scode[e + 1] & kE)) {
+      gub -= P(c0)[e + 1];
+      gvx -= P(c2)[e + 1];
+      gvy -= P(c5)[e + 1];
+    }
+    if (scode[e - WX] & kS) {
+      gub += P(c1)[e - WX];
+      gvx += P(c4)[e - WX];
+      gvy += P(c3)[e - WX];
+    }
+    if (!(scode[e + WX] & kS)) {
+      gub -= P(c1)[e + WX];
+      gvx -= P(c4)[e + WX];
+      gvy -= P(c3)[e + WX];
+    }
+    G0UB[f] = gub;
+    G0VX[f] = gvx;
+    G0VY[f] = gvy;
+  }
+  block_sum_to<3>(acc, r.scal + G_LAMBDA);
+}
+
+// Tile shapes of the reverse step, selected by vfs_grad_set_options.
+#define VFS_REV_SHAPES(X) \
+  X(1, 32, 16, 512)       \
+  X(2, 32, 8, 256)        \
+  X(3, 64, 8, 512)        \
+  X(4, 32, 32, 1024)      \
+  X(5, 28, 16, 640)
+
+cudaError_t launch_rev_tile(int shape, const RevArgs& r, cudaStream_t s) {
+  switch (shape) {
+#define VFS_REV_L(id, TX, TY, NT)                                                      \
+  case id: {                                                                           \
+    dim3 grid((r.w + TX - 1) / TX, (r.h + TY - 1) / TY);                               \
+    k_rev_tile<TX, TY, NT><<<grid, NT, RevGeom<TX, TY>::smem_bytes(), s>>>(r);         \
+    return cudaGetLastError();                                                         \
+  }
+    VFS_REV_SHAPES(VFS_REV_L)
+#undef VFS_REV_L
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t prepare_rev_tile() {
+  cudaError_t e = cudaSuccess;
+#define VFS_REV_P(id, TX, TY, NT)                                                                         \
+  if (e == cudaSuccess)                                                                                   \
+    e = cudaFuncSetAttribute(k_rev_tile<TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                             (int)RevGeom<TX, TY>::smem_bytes());
+  VFS_REV_SHAPES(VFS_REV_P)
+#undef VFS_REV_P
+  return e;
+}
+
+bool rev_shape_ok(int shape) {
+  switch (shape) {
+#define VFS_REV_OK(id, TX, TY, NT) \
+  case id: return true;
+    VFS_REV_SHAPES(VFS_REV_OK)
+#undef VFS_REV_OK
+    default: return false;
+  }
+}
+
 // ---------------------------------------------------------------- warp prologue reversed
 // computeDerivatives (Python/vfs.cu:120-142, 304-324) reversed: the
 // cotangents of (Iu, Iz) go to the reference level image, the warped image
@@ -807,6 +1199,9 @@ struct VfsGradPlan {
   std::vector<float*> gref, gother;
   std::vector<float2*> gtvf;
   double* scal = nullptr;
+  TgvState* d_slot = nullptr;  // device copy of `slot` (recording targets)
+  int fused_reverse = 1;  // reverse-step tile shape, 0: three gather kernels
+  int trace_variant = 0;  // 0: the level's forward variant if it records, else 134
 };
 
 namespace {
@@ -888,6 +1283,7 @@ size_t grad_layout(VfsGradPlan* gp, const VfsParams* p, char* base) {
     gp->gtvf[l] = cv.take<float2>(n * 8);
   }
   gp->scal = cv.take<double>(G_NSCAL * sizeof(double));
+  gp->d_slot = cv.take<TgvState>((gp->ckpt + 1) * sizeof(TgvState));
   return cv.off + kGAlign;
 }
 
@@ -1045,7 +1441,14 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
     cst.code = v.code;
     VFS_TRY_CUDA(launch_tensor_soa(cst, v.code, v.smooth_tex, mask, pl->kc, h, w, s), "tensor");
     for (int q = 0; q < 6; ++q) VFS_TRY_CUDA(zero(gp->gcp[q], n * 4, s), "memset");
-    const int var1 = 1;  // one iteration per launch for the recomputation
+    // recording kernel for the recomputation (0: one iteration per launch)
+    int tv = gp->trace_variant;
+    if (tv == 0) {
+      const int fv = level_variant_of(pl, l);
+      tv = tgv_has_trace(fv) ? fv : 134;
+    } else if (tv < 0 || !tgv_has_trace(tv)) {
+      tv = 0;
+    }
     for (int wi = nW - 1; wi >= 0; --wi) {
       auto& wt = gp->tape[l][wi];
       // the warp's tvec, warped image, derivatives and initial state
@@ -1063,10 +1466,18 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
         const int nj = std::max(0, std::min(gp->ckpt, nI - it0));
         std::vector<TgvState> S(nj + 1);
         S[0] = j == 0 ? gp->slot[0] : wt.ck[j - 1];
-        for (int q = 1; q <= nj; ++q) {
-          S[q] = gp->slot[q];
-          VFS_TRY_CUDA(launch_tgv_block(var1, S[q - 1], S[q], cst, pl->sched, it0 + q - 1, 1, pl->kc, h, w, s),
-                       "tgv recompute");
+        for (int q = 1; q <= nj; ++q) S[q] = gp->slot[q];
+        if (tv) {
+          for (int q = 0; q < nj;) {
+            const int m = std::min(tgv_max_iters_per_launch(tv), nj - q);
+            VFS_TRY_CUDA(launch_tgv_trace(tv, S[q], gp->d_slot + q + 1, cst, pl->sched, it0 + q, m, pl->kc, h, w, s),
+                         "tgv recompute");
+            q += m;
+          }
+        } else {
+          for (int q = 1; q <= nj; ++q)
+            VFS_TRY_CUDA(launch_tgv_block(1, S[q - 1], S[q], cst, pl->sched, it0 + q - 1, 1, pl->kc, h, w, s),
+                         "tgv recompute");
         }
         if (j == gp->nint - 1) {
           // cotangent of the final state: u from the median/clamp, u_ from
@@ -1083,10 +1494,14 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
           r.s1 = S[q + 1];
           r.g1 = gp->G[gi];
           r.g0 = gp->G[gi ^ 1];
-          k_rev1<<<g2d(h, w), kGB, 0, s>>>(r);
-          k_rev2<<<g2d(h, w), kGB, 0, s>>>(r);
-          k_rev3<<<g2d(h, w), kGB, 0, s>>>(r);
-          VFS_TRY_CUDA(cudaGetLastError(), "tgv backward");
+          if (gp->fused_reverse) {
+            VFS_TRY_CUDA(launch_rev_tile(gp->fused_reverse, r, s), "tgv backward");
+          } else {
+            k_rev1<<<g2d(h, w), kGB, 0, s>>>(r);
+            k_rev2<<<g2d(h, w), kGB, 0, s>>>(r);
+            k_rev3<<<g2d(h, w), kGB, 0, s>>>(r);
+            VFS_TRY_CUDA(cudaGetLastError(), "tgv backward");
+          }
           gi ^= 1;
         }
       }
@@ -1189,6 +1604,12 @@ int vfs_grad_create(const VfsParams* prm, int ckpt_every, float f, float u0, flo
   step_schedule(prm->nSolverIters, prm->timeStepLambda, gp->sched.data());
   char* gbase = reinterpret_cast<char*>(gru(reinterpret_cast<uintptr_t>(base + gru(pb, kGAlign)), kGAlign));
   grad_layout(gp, prm, gbase);
+  cudaError_t e = cudaMemcpy(gp->d_slot, gp->slot.data(), gp->slot.size() * sizeof(TgvState), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = prepare_rev_tile();
+  if (e != cudaSuccess) {
+    vfs_grad_destroy(gp);
+    return cuda_status(e, "gradient plan setup");
+  }
   *out = gp;
   return VFS_OK;
 }
@@ -1201,6 +1622,16 @@ int vfs_grad_destroy(VfsGradPlan* gp) {
 }
 
 VfsPlan* vfs_grad_plan(VfsGradPlan* gp) { return gp ? gp->pl : nullptr; }
+
+int vfs_grad_set_options(VfsGradPlan* gp, int fused_reverse, int trace_variant) {
+  if (!gp) return fail(VFS_ERR_ARG, "plan is NULL");
+  if (trace_variant > 0 && !tgv_has_trace(trace_variant))
+    return fail(VFS_ERR_ARG, "variant has no recording form");
+  if (fused_reverse != 0 && !rev_shape_ok(fused_reverse)) return fail(VFS_ERR_ARG, "unknown reverse tile shape");
+  gp->fused_reverse = fused_reverse;
+  gp->trace_variant = trace_variant;
+  return VFS_OK;
+}
 
 int vfs_grad_forward(VfsGradPlan* gp, const float* img_ref, const float* img_other, const double* t,
                      const double* theta, float* depth_out, void* stream) {

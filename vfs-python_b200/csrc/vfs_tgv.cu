@@ -290,6 +290,15 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   X(216, reg, 5, 16, 16, 1024)       \
   X(217, reg, 6, 14, 14, 1024)
 
+// Register-owned variants also compiled in recording form (every
+// iteration's state written out), for the reverse mode's recomputation.
+#define VFS_TGV_TRACE_VARIANTS(X) \
+  X(124, 4, 32, 16, 256)          \
+  X(134, 4, 32, 32, 1024)         \
+  X(207, 4, 8, 8, 416)            \
+  X(212, 4, 20, 20, 1024)         \
+  X(216, 5, 16, 16, 1024)
+
 }  // namespace
 
 cudaError_t tgv_prepare() {
@@ -298,7 +307,42 @@ cudaError_t tgv_prepare() {
   if (e == cudaSuccess) e = prepare_##impl<K, TX, TY, NT>();
   VFS_TGV_VARIANTS(VFS_PREP)
 #undef VFS_PREP
+#define VFS_PREP_T(id, K, TX, TY, NT)                                                                      \
+  if (e == cudaSuccess)                                                                                    \
+    e = cudaFuncSetAttribute(k_tgv_reg_trace<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             (int)RegGeom<K, TX, TY>::smem_bytes());
+  VFS_TGV_TRACE_VARIANTS(VFS_PREP_T)
+#undef VFS_PREP_T
   return e;
+}
+
+bool tgv_has_trace(int variant) {
+  switch (variant) {
+#define VFS_HAS_T(id, K, TX, TY, NT) \
+  case id: return true;
+    VFS_TGV_TRACE_VARIANTS(VFS_HAS_T)
+#undef VFS_HAS_T
+    default: return false;
+  }
+}
+
+cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState* trace, const TgvConsts& c,
+                             const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
+                             cudaStream_t s) {
+  if (h <= 0 || w <= 0 || niter <= 0) return cudaSuccess;
+  switch (variant) {
+#define VFS_LAUNCH_T(id, K, TX, TY, NT)                                                                    \
+  case id: {                                                                                               \
+    if (niter > K) return cudaErrorInvalidValue;                                                           \
+    dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);                                                       \
+    k_tgv_reg_trace<K, TX, TY, NT><<<grid, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(in, trace, c, sched, it0, \
+                                                                                       niter, kc, h, w);   \
+    return cudaGetLastError();                                                                             \
+  }
+    VFS_TGV_TRACE_VARIANTS(VFS_LAUNCH_T)
+#undef VFS_LAUNCH_T
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 int tgv_max_iters_per_launch(int variant) {

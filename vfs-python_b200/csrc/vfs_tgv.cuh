@@ -55,6 +55,14 @@ cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& ou
                              const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
                              cudaStream_t s);
 
+// Recording form of a register-owned variant (tgv_has_trace): runs `niter`
+// (<= K) iterations from `in` and writes the state after iteration s to
+// trace[s - 1] (an array of state sets in device memory).
+bool tgv_has_trace(int variant);
+cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState* trace, const TgvConsts& c,
+                             const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
+                             cudaStream_t s);
+
 // Cluster-resident solve of a whole level (vfs_tgv_cluster.cu): all `niter`
 // iterations, then median filter and clamped flow update, in one launch of a
 // `cluster`-CTA cluster.  tgv_cluster_size returns the cluster size to use for

@@ -25,10 +25,13 @@ struct RegGeom {
 };
 
 // One CTA's tile whose origin is (x0, y0).
-template <int K, int TX, int TY, int NT>
+// With TRACE, the state after iteration s (of this launch) is written to
+// trace[s - 1] instead of the final state to `out`.
+template <int K, int TX, int TY, int NT, bool TRACE = false>
 __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState& out, const TgvConsts& cst,
                                              const float3* __restrict__ sched, int it0, int niter,
-                                             const SolverConsts& kc, int h, int w, int x0, int y0) {
+                                             const SolverConsts& kc, int h, int w, int x0, int y0,
+                                             const TgvState* __restrict__ trace = nullptr) {
   using G = RegGeom<K, TX, TY>;
   constexpr int WX = G::WX, N = G::N, J = (N + NT - 1) / NT;
   extern __shared__ float4 smem_raw[];
@@ -146,10 +149,33 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
         sVY[i] = vo.y;
       }
     }
+    if constexpr (TRACE) {  // each thread writes the tile pixels it owns
+      const TgvState o = trace[s - 1];
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int tx = rwx[j] - 2 * K, ty = rwy[j] - 2 * K;
+        if (tx < 0 || tx >= TX || ty < 0 || ty >= TY) continue;
+        const int X = x0 + tx, Y = y0 + ty;
+        if (X >= w || Y >= h) continue;
+        const int i = threadIdx.x + j * NT;
+        const long f = (long)Y * w + X;
+        o.u[f] = ru[j];
+        o.ub[f] = sUB[i];
+        o.vbx[f] = sVX[i];
+        o.vby[f] = sVY[i];
+        o.px[f] = rpx[j];
+        o.py[f] = rpy[j];
+        o.qx[f] = sQX[i];
+        o.qy[f] = sQY[i];
+        o.qz[f] = sQZ[i];
+        o.qw[f] = sQW[i];
+      }
+    }
     __syncthreads();
   }
 
   // ---- write back the tile (real pixels only)
+  if constexpr (!TRACE) {
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int tx = rwx[j] - 2 * K, ty = rwy[j] - 2 * K;
@@ -169,6 +195,7 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     out.qz[f] = sQZ[i];
     out.qw[f] = sQW[i];
   }
+  }
 }
 
 template <int K, int TX, int TY, int NT>
@@ -176,6 +203,15 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
     k_tgv_reg(TgvState in, TgvState out, TgvConsts cst, const float3* __restrict__ sched, int it0, int niter,
               SolverConsts kc, int h, int w) {
   tgv_reg_tile<K, TX, TY, NT>(in, out, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY);
+}
+
+// Recording: every iteration's state to trace[0..niter).
+template <int K, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
+    k_tgv_reg_trace(TgvState in, const TgvState* __restrict__ trace, TgvConsts cst, const float3* __restrict__ sched,
+                    int it0, int niter, SolverConsts kc, int h, int w) {
+  tgv_reg_tile<K, TX, TY, NT, true>(in, in, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY,
+                                    trace);
 }
 
 // Batched: one launch over the tiles of many images (the pairs of a batch at

@@ -120,6 +120,7 @@ _SIGS = {
     "vfs_grad_plan": [_P],
     "vfs_grad_forward": [_P, _P, _P, _P, _P, _P, _P],
     "vfs_grad_backward": [_P, _P, _P, _P, _P, _P],
+    "vfs_grad_set_options": [_P, _I, _I],
 }
 
 _lib = None

@@ -61,6 +61,12 @@ class DepthSolver:
         self._generation = 0
         self._recorded = None
 
+    def set_options(self, fused_reverse: int = 1, trace_variant: int = 0) -> None:
+        """Backward kernel forms: the tile shape of the one-kernel reverse step
+        (1..5; 0: three gather kernels) and the TGV variant recomputing
+        checkpoint intervals (0 automatic, -1 one iteration per launch)."""
+        call("vfs_grad_set_options", self._gp, int(fused_reverse), int(trace_variant))
+
     def theta_of(self, param=None) -> torch.Tensor:
         p = param or self.param
         return torch.tensor([float(getattr(p, k)) for k in THETA], dtype=torch.float64)
