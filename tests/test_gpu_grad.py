@@ -98,7 +98,7 @@ def test_grad_independent_of_checkpoint_spacing():
     good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
     wts = np.where(good, np.random.default_rng(1).normal(0, 1, good.shape), 0.0) * 1e-3
     outs = []
-    for ck in (1, 4, 9, 100):
+    for ck in (1, 2, 4, 9, 100):
         s = _solver(P, prm, ckpt=ck)
         outs.append(_gpu_grads(s, I0, I1, t, theta, wts))
         s.release()
@@ -143,9 +143,15 @@ def test_backward_kernel_forms_agree():
     good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
     wts = np.where(good, np.random.default_rng(2).normal(0, 1, good.shape), 0.0) * 1e-3
     outs = []
-    for fused, tv in ((0, -1), (1, -1), (0, 0), (1, 0), (1, 124), (1, 216), (2, 0), (3, 0), (4, 0), (5, 0)):
+    forms = [(0, -1), (1, -1), (0, 0), (1, 0), (1, 124), (1, 216), (2, 0), (3, 0), (4, 0), (5, 0)]
+    forms += [(b, 0) for b in (11, 12, 13, 14, 15, 16)]
+    for fused, tv in forms:
         s.set_options(fused, tv)
         outs.append(_gpu_grads(s, I0, I1, t, theta, wts))
+    s1 = _solver(P, prm, ckpt=1)  # every state recorded, no recomputation
+    for fused in (1, 11, 14, 16):
+        s1.set_options(fused, 0)
+        outs.append(_gpu_grads(s1, I0, I1, t, theta, wts))
     for o in outs[1:]:
         for a, b in zip(o[1:], outs[0][1:]):
             assert _rel(a, b) < 1e-5

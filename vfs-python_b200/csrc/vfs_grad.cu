@@ -568,10 +568,6 @@ __global__ void __launch_bounds__(NT) k_rev_tile(RevArgs r) {
   const float* __restrict__ const S0QY = r.s0.qy;
   const float* __restrict__ const S0QZ = r.s0.qz;
   const float* __restrict__ const S0QW = r.s0.qw;
-  const float* __restrict__ const S1U = r.s1.u;
-  const float* __restrict__ const S1UB = r.s1.ub;
-  const float* __restrict__ const S1VX = r.s1.vbx;
-  const float* __restrict__ const S1VY = r.s1.vby;
   const float* __restrict__ const S1PX = r.s1.px;
   const float* __restrict__ const S1PY = r.s1.py;
   const float* __restrict__ const S1QX = r.s1.qx;
@@ -921,6 +917,467 @@ bool rev_shape_ok(int shape) {
   }
 }
 
+// ---------------------------------------------------------------- blocked reverse
+// k (<= K) reverse iterations per launch: from the cotangent of S_{i0+k} to
+// that of S_{i0}, reading the recorded states S_{i0} .. S_{i0+k}.  The same
+// three phases per step as k_rev_tile; the cotangent state stays in the
+// registers of the thread that owns its window pixel and the constant
+// cotangents accumulate in shared memory, so cotangents and constants cross
+// HBM once per launch instead of once per iteration.  The recorded states
+// stream into three shared-memory buffers with cp.async: while step m runs
+// on S_{i0+k-m} and S_{i0+k-m+1}, the state of step m+1 is already loading.
+//
+// Geometry.  Step m (1..k) produces a valid cotangent on O_m = [-(k-m),
+// T + 2(k-m)) in tile coordinates (phase 3 there; phase 2 on O_m grown by 1,
+// phase 1 on O_m grown by 1 low and 2 high) and reads S_{i0+k-m} on O_m
+// grown by 2, so the window is the tile plus K+1 pixels low and 2K high, in
+// the flat addressing of k_rev_tile.
+//
+// Quotients that only scale cotangents use the fast divide; tau / eta uses a
+// reciprocal of eta formed once per launch (the branch of the L1 shrink is
+// the forward's except where rho is within an ulp of the bound).
+struct RevBlockArgs {
+  const TgvState* states;  // states[0..k]: S_{i0} .. S_{i0+k}
+  TgvState g_in, g_out;    // cotangent of S_{i0+k} (in), of S_{i0} (out)
+  TgvConsts c;
+  float* gc[8];
+  const float3* sched;
+  int i0, niter;
+  SolverConsts k;
+  int h, w;
+  double* scal;
+};
+
+// state buffer planes
+enum { sUB, sVX, sVY, sU, sPX, sPY, sQX, sQY, sQZ, sQW, kStPlanes };
+enum RbPlane { bS0 = 0, bAX = 3 * kStPlanes, bAY, bAB, bC0, bCA = bC0 + 6, bCB, bCC, bREX, bREY, bREZ, bIU, bIZ,
+               kRbPlanes };
+
+template <int K, int TX, int TY>
+struct RbGeom {
+  static constexpr int LH = K + 1;
+  static constexpr int WX = TX + 3 * K + 1, WY = TY + 3 * K + 1, N = WX * WY;
+  static constexpr size_t smem_bytes() {
+    return (size_t)kRbPlanes * N * 4 + (size_t)8 * TX * TY * 4 + ((N + 15) / 16) * 16;
+  }
+};
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NG>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NG) : "memory"); }
+
+template <int K, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
+  using G = RbGeom<K, TX, TY>;
+  constexpr int WX = G::WX, N = G::N, LH = G::LH, J = (N + NT - 1) / NT, TT = TX * TY;
+  extern __shared__ float4 smem_raw[];
+  float* const sm = reinterpret_cast<float*>(smem_raw);
+  float* const sgc = sm + (size_t)kRbPlanes * N;
+  uint8_t* const scode = reinterpret_cast<uint8_t*>(sgc + 8 * TT);
+  auto P = [&](int plane) { return sm + (size_t)plane * N; };
+  const int w = r.w, h = r.h;
+  const long n = (long)h * w;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const long base = (long)(y0 - LH) * w + (x0 - LH);
+  const int k = r.niter < K ? r.niter : K;
+  const float eps = 1E-7f;
+  const float al0 = r.k.alpha0, al1 = r.k.alpha1, lam = r.k.lambda;
+  float acc[3] = {0.f, 0.f, 0.f};  // Lambda, alpha0, alpha1
+
+  float gU[J], gUB[J], gVX[J], gVY[J], gPX[J], gPY[J], gQ0[J], gQ1[J], gQ2[J], gQ3[J];
+  int rx[J], ry[J];
+
+  // state S_{i0+q} into buffer b over O_m grown by 2 (m = k - q; the whole
+  // window for q = k)
+  auto load_state = [&](int q, int b) {
+    const TgvState S = r.states[q];
+    const float* src[kStPlanes] = {S.ub, S.vbx, S.vby, S.u, S.px, S.py, S.qx, S.qy, S.qz, S.qw};
+    const int m = k - q;
+    const int lo = m == 0 ? -LH : -(k - m) - 2, hiX = m == 0 ? TX + 2 * K : TX + 2 * (k - m) + 2,
+              hiY = m == 0 ? TY + 2 * K : TY + 2 * (k - m) + 2;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      if (rx[j] < lo || rx[j] >= hiX || ry[j] < lo || ry[j] >= hiY) continue;
+      const int e = threadIdx.x + j * NT;
+      const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LH);
+      const bool ok = f >= 0 && f < n;
+#pragma unroll
+      for (int pl = 0; pl < kStPlanes; ++pl) cp_async4(P(bS0 + b * kStPlanes + pl) + e, ok ? src[pl] + f : src[pl], ok);
+    }
+    cp_async_commit();
+  };
+
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int e = threadIdx.x + j * NT;
+    const int wy = e / WX, wx = e - wy * WX;
+    rx[j] = wx - LH;
+    ry[j] = e < N ? wy - LH : (1 << 20);
+  }
+  load_state(k, 0);
+  if (k >= 1) load_state(k - 1, 1);
+  if (k >= 2) load_state(k - 2, 2);
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int e = threadIdx.x + j * NT;
+    const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LH);
+    const bool ok = e < N && f >= 0 && f < n;
+    gU[j] = ok ? r.g_in.u[f] : 0.f;
+    gUB[j] = ok ? r.g_in.ub[f] : 0.f;
+    gVX[j] = ok ? r.g_in.vbx[f] : 0.f;
+    gVY[j] = ok ? r.g_in.vby[f] : 0.f;
+    gPX[j] = ok ? r.g_in.px[f] : 0.f;
+    gPY[j] = ok ? r.g_in.py[f] : 0.f;
+    gQ0[j] = ok ? r.g_in.qx[f] : 0.f;
+    gQ1[j] = ok ? r.g_in.qy[f] : 0.f;
+    gQ2[j] = ok ? r.g_in.qz[f] : 0.f;
+    gQ3[j] = ok ? r.g_in.qw[f] : 0.f;
+    if (e < N) {
+      P(bCA)[e] = ok ? r.c.a[f] : 0.f;
+      P(bCB)[e] = ok ? r.c.b[f] : 0.f;
+      P(bCC)[e] = ok ? r.c.c[f] : 0.f;
+      const float ex = ok ? r.c.ex[f] : 0.f, ey = ok ? r.c.ey[f] : 0.f, ez = ok ? r.c.ez[f] : 0.f;
+      P(bREX)[e] = fabsf(ex) < eps ? 0.f : 1.f / ex;
+      P(bREY)[e] = fabsf(ey) < eps ? 0.f : 1.f / ey;
+      P(bREZ)[e] = fabsf(ez) < eps ? 0.f : 1.f / ez;
+      P(bIU)[e] = ok ? r.c.iu[f] : 0.f;
+      P(bIZ)[e] = ok ? r.c.iz[f] : 0.f;
+      scode[e] = ok ? r.c.code[f] : 0;
+    }
+  }
+  for (int q = threadIdx.x; q < 8 * TT; q += NT) sgc[q] = 0.f;
+  if (k >= 2) cp_async_wait<1>(); else cp_async_wait<0>();
+  __syncthreads();
+
+  for (int m = 1; m <= k; ++m) {
+    const float3 ss = r.sched[r.i0 + k - m];
+    const float sigma = ss.x, tau = ss.y, mu = ss.z;
+    const int lo = -(k - m), hiX = TX + 2 * (k - m), hiY = TY + 2 * (k - m);
+    const int L0 = bS0 + (m % 3) * kStPlanes, H0 = bS0 + ((m - 1) % 3) * kStPlanes;  // later / earlier state
+    // phase 1: primal and threshold reversed on [lo - 1, hi + 2)
+    float nU[J], lUB[J], lVX[J], lVY[J];
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      nU[j] = lUB[j] = lVX[j] = lVY[j] = 0.f;
+      if (rx[j] < lo - 1 || rx[j] >= hiX + 2 || ry[j] < lo - 1 || ry[j] >= hiY + 2) continue;
+      const int e = threadIdx.x + j * NT;
+      const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LH);
+      const uint8_t c = scode[e];
+      const bool core = rx[j] >= 0 && rx[j] < TX && ry[j] >= 0 && ry[j] < TY && x0 + rx[j] < w && y0 + ry[j] < h;
+      float Ax = 0.f, Ay = 0.f, Bv = 0.f;
+      if (f >= 0 && f < n && (c & kSelf)) {
+        const float gubn = gUB[j], gvbx = gVX[j], gvby = gVY[j];
+        const float gun = gU[j] + (1.f + mu) * gubn;
+        const float gVx = (1.f + mu) * gvbx, gVy = (1.f + mu) * gvby;
+        const float* hq = P(H0 + sQX);
+        const float gQx = ((c & kE) ? hq[e] : 0.f) - ((c & kW) ? hq[e - 1] : 0.f);
+        const float gQw = ((c & kE) ? P(H0 + sQW)[e] : 0.f) - ((c & kW) ? P(H0 + sQW)[e - 1] : 0.f);
+        const float gQy = ((c & kS) ? P(H0 + sQY)[e] : 0.f) - ((c & kN) ? P(H0 + sQY)[e - WX] : 0.f);
+        const float gQz = ((c & kS) ? P(H0 + sQZ)[e] : 0.f) - ((c & kN) ? P(H0 + sQZ)[e - WX] : 0.f);
+        const float a = P(bCA)[e], b = P(bCB)[e], cc = P(bCC)[e];
+        const float px = P(H0 + sPX)[e], py = P(H0 + sPY)[e];
+        const float tpx = fmaf(a, px, cc * py), tpy = fmaf(cc, px, b * py);
+        const float tpWx = fmaf(P(bCA)[e - 1], P(H0 + sPX)[e - 1], P(bCC)[e - 1] * P(H0 + sPY)[e - 1]);
+        const float tpNy = fmaf(P(bCC)[e - WX], P(H0 + sPX)[e - WX], P(bCB)[e - WX] * P(H0 + sPY)[e - WX]);
+        const float rex = P(bREX)[e], rey = P(bREY)[e], rez = P(bREZ)[e];
+        const float t1 = rey == 0.f ? tau : tau * rey, t2 = rez == 0.f ? tau : tau * rez;
+        Ax = t1 * al0 * gVx;
+        Ay = t2 * al0 * gVy;
+        const bool E_ = c & kE, W_ = c & kW, S_ = c & kS, N_ = c & kN;
+        const float gTx = (E_ && W_) ? tpx - tpWx : (!E_ ? -tpWx : tpx);
+        const float gTy = (S_ && N_) ? tpy - tpNy : (!S_ ? -tpNy : tpy);
+        const float Iu = P(bIU)[e], Iz = P(bIZ)[e];
+        const float te = rex == 0.f ? tau : tau * rex;
+        const float u = P(L0 + sU)[e], ub = P(L0 + sUB)[e];
+        const float ut = ub + te * (gTx + gTy);
+        const float rho = Iu * (ut - u) + Iz;
+        const float Bd = lam * te * Iu * Iu;
+        float gu = 0.f, gut = 0.f, gte = 0.f, giu = 0.f, giz = 0.f, gl = 0.f;
+        if ((rho <= Bd) && (rho >= -Bd)) {
+          if (fabsf(Iu) >= eps) {
+            const float ri = __fdividef(1.f, Iu);
+            gu = gun;
+            giz = -gun * ri;
+            giu = gun * Iz * ri * ri;
+          } else {
+            gut = gun;
+          }
+        } else if (rho < -Bd) {
+          gut = gun;
+          gl = te * Iu * gun;
+          gte = lam * Iu * gun;
+          giu = lam * te * gun;
+        } else if (rho > Bd) {
+          gut = gun;
+          gl = -te * Iu * gun;
+          gte = -lam * Iu * gun;
+          giu = -lam * te * gun;
+        } else {
+          gu = gun;
+        }
+        gte += (gTx + gTy) * gut;
+        Bv = te * gut;
+        nU[j] = gu;
+        lUB[j] = -mu * gubn + gut;
+        lVX[j] = gVx - mu * gvbx;
+        lVY[j] = gVy - mu * gvby;
+        if (core) {
+          const int ci = ry[j] * TX + rx[j];
+          const float inx = fmaf(al1, tpx, al0 * (gQx + gQz));
+          const float iny = fmaf(al1, tpy, al0 * (gQw + gQy));
+          sgc[3 * TT + ci] -= te * rex * gte;
+          sgc[4 * TT + ci] -= t1 * rey * inx * gVx;
+          sgc[5 * TT + ci] -= t2 * rez * iny * gVy;
+          sgc[6 * TT + ci] += giu;
+          sgc[7 * TT + ci] += giz;
+          acc[0] += gl;
+          acc[1] += t1 * (gQx + gQz) * gVx + t2 * (gQw + gQy) * gVy;
+          acc[2] += t1 * tpx * gVx + t2 * tpy * gVy;
+        }
+      }
+      P(bAX)[e] = Ax;
+      P(bAY)[e] = Ay;
+      P(bAB)[e] = Bv;
+    }
+    __syncthreads();
+    // phase 2: dual step reversed on [lo - 1, hi + 1)
+    float nPX[J], nPY[J], nQ0[J], nQ1[J], nQ2[J], nQ3[J];
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      nPX[j] = nPY[j] = nQ0[j] = nQ1[j] = nQ2[j] = nQ3[j] = 0.f;
+      if (rx[j] < lo - 1 || rx[j] >= hiX + 1 || ry[j] < lo - 1 || ry[j] >= hiY + 1) continue;
+      const int e = threadIdx.x + j * NT;
+      const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LH);
+      const uint8_t c = scode[e];
+      const bool core = rx[j] >= 0 && rx[j] < TX && ry[j] >= 0 && ry[j] < TY && x0 + rx[j] < w && y0 + ry[j] < h;
+      float Cv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (f >= 0 && f < n && (c & kSelf)) {
+        const uint8_t cE = scode[e + 1], cS = scode[e + WX];
+        const float Bv = P(bAB)[e];
+        const float gVx = (1.f + mu) * gVX[j], gVy = (1.f + mu) * gVY[j];
+        const float rey = P(bREY)[e], rez = P(bREZ)[e];
+        const float t1 = rey == 0.f ? tau : tau * rey, t2 = rez == 0.f ? tau : tau * rez;
+        const float gtpx = t1 * al1 * gVx + ((c & kE) ? Bv : 0.f) - (((cE & kW) || !(cE & kE)) ? P(bAB)[e + 1] : 0.f);
+        const float gtpy = t2 * al1 * gVy + ((c & kS) ? Bv : 0.f) - (((cS & kN) || !(cS & kS)) ? P(bAB)[e + WX] : 0.f);
+        const float Ax = P(bAX)[e], Ay = P(bAY)[e];
+        float gq0 = gQ0[j] + ((c & kE) ? Ax : 0.f) - ((cE & kW) ? P(bAX)[e + 1] : 0.f);
+        float gq3 = gQ3[j] + ((c & kE) ? Ay : 0.f) - ((cE & kW) ? P(bAY)[e + 1] : 0.f);
+        float gq1 = gQ1[j] + ((c & kS) ? Ay : 0.f) - ((cS & kN) ? P(bAY)[e + WX] : 0.f);
+        float gq2 = gQ2[j] + ((c & kS) ? Ax : 0.f) - ((cS & kN) ? P(bAX)[e + WX] : 0.f);
+        const float a = P(bCA)[e], b = P(bCB)[e], cc = P(bCC)[e];
+        const float pnx = P(H0 + sPX)[e], pny = P(H0 + sPY)[e];
+        const float gpx = gPX[j] + fmaf(a, gtpx, cc * gtpy);
+        const float gpy = gPY[j] + fmaf(cc, gtpx, b * gtpy);
+        const float ga = pnx * gtpx, gb = pny * gtpy, gcc = pny * gtpx + pnx * gtpy;
+        const float* lub = P(L0 + sUB);
+        const float* lvx = P(L0 + sVX);
+        const float* lvy = P(L0 + sVY);
+        const float uc = lub[e], vcx = lvx[e], vcy = lvy[e];
+        float gUx, gUy, gVxx, gVyy, gVz, gVw;
+        if (c & kE) {
+          gUx = lub[e + 1] - uc - vcx;
+          gVxx = lvx[e + 1] - vcx;
+          gVw = lvy[e + 1] - vcy;
+        } else {
+          gUx = uc - lub[e - 1] - vcx;
+          gVxx = vcx - lvx[e - 1];
+          gVw = vcy - lvy[e - 1];
+        }
+        if (c & kS) {
+          gUy = lub[e + WX] - uc - vcy;
+          gVyy = lvy[e + WX] - vcy;
+          gVz = lvx[e + WX] - vcx;
+        } else {
+          gUy = uc - lub[e - WX] - vcy;
+          gVyy = vcy - lvy[e - WX];
+          gVz = vcx - lvx[e - WX];
+        }
+        const float scaleP = al1 * sigma / r.k.etaP;
+        const float scaleQ = al0 * sigma / r.k.etaQ;
+        const float tux = fmaf(a, gUx, cc * gUy), tuy = fmaf(cc, gUx, b * gUy);
+        const float upx = fmaf(scaleP, tux, P(L0 + sPX)[e]), upy = fmaf(scaleP, tuy, P(L0 + sPY)[e]);
+        const float nP = hypotf(upx, upy);
+        float gP0 = gpx, gP1 = gpy;
+        if (nP > 1.f) {
+          const float dt = pnx * gpx + pny * gpy, rn = __fdividef(1.f, nP);
+          gP0 = (gpx - pnx * dt) * rn;
+          gP1 = (gpy - pny * dt) * rn;
+        }
+        const float uq0 = fmaf(scaleQ, gVxx, P(L0 + sQX)[e]), uq1 = fmaf(scaleQ, gVyy, P(L0 + sQY)[e]);
+        const float uq2 = fmaf(scaleQ, gVz, P(L0 + sQZ)[e]), uq3 = fmaf(scaleQ, gVw, P(L0 + sQW)[e]);
+        const float nQ = norm4df(uq0, uq1, uq2, uq3);
+        if (nQ > 1.f) {
+          const float q0 = P(H0 + sQX)[e], q1 = P(H0 + sQY)[e], q2 = P(H0 + sQZ)[e], q3 = P(H0 + sQW)[e];
+          const float dt = q0 * gq0 + q1 * gq1 + q2 * gq2 + q3 * gq3, rn = __fdividef(1.f, nQ);
+          gq0 = (gq0 - q0 * dt) * rn;
+          gq1 = (gq1 - q1 * dt) * rn;
+          gq2 = (gq2 - q2 * dt) * rn;
+          gq3 = (gq3 - q3 * dt) * rn;
+        }
+        const float gtux = scaleP * gP0, gtuy = scaleP * gP1;
+        Cv[0] = fmaf(a, gtux, cc * gtuy);
+        Cv[1] = fmaf(cc, gtux, b * gtuy);
+        Cv[2] = scaleQ * gq0;
+        Cv[3] = scaleQ * gq1;
+        Cv[4] = scaleQ * gq2;
+        Cv[5] = scaleQ * gq3;
+        nPX[j] = gP0;
+        nPY[j] = gP1;
+        nQ0[j] = gq0;
+        nQ1[j] = gq1;
+        nQ2[j] = gq2;
+        nQ3[j] = gq3;
+        if (core) {
+          const int ci = ry[j] * TX + rx[j];
+          sgc[0 * TT + ci] += ga + gUx * gtux;
+          sgc[1 * TT + ci] += gb + gUy * gtuy;
+          sgc[2 * TT + ci] += gcc + gUy * gtux + gUx * gtuy;
+          acc[1] += sigma / r.k.etaQ * (gVxx * gq0 + gVyy * gq1 + gVz * gq2 + gVw * gq3);
+          acc[2] += sigma / r.k.etaP * (tux * gP0 + tuy * gP1);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 6; ++q) P(bC0 + q)[e] = Cv[q];
+    }
+    __syncthreads();
+    // phase 3: transposed gradients of u_ and v_ on [lo, hi); commit the step
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      if (rx[j] < lo || rx[j] >= hiX || ry[j] < lo || ry[j] >= hiY) continue;
+      const int e = threadIdx.x + j * NT;
+      const uint8_t c = scode[e];
+      float gub = lUB[j], gvx = lVX[j], gvy = lVY[j];
+      if (c & kSelf) {
+        const float u0 = P(bC0)[e], u1 = P(bC0 + 1)[e];
+        const float v0 = P(bC0 + 2)[e], v1 = P(bC0 + 3)[e], v2 = P(bC0 + 4)[e], v3 = P(bC0 + 5)[e];
+        gub += ((c & kE) ? -u0 : u0) + ((c & kS) ? -u1 : u1);
+        gvx += -u0 + ((c & kE) ? -v0 : v0) + ((c & kS) ? -v2 : v2);
+        gvy += -u1 + ((c & kE) ? -v3 : v3) + ((c & kS) ? -v1 : v1);
+      }
+      if (scode[e - 1] & kE) {
+        gub += P(bC0)[e - 1];
+        gvx += P(bC0 + 2)[e - 1];
+        gvy += P(bC0 + 5)[e - 1];
+      }
+      if (!(scode[e + 1] & kE)) {
+        gub -= P(bC0)[e + 1];
+        gvx -= P(bC0 + 2)[e + 1];
+        gvy -= P(bC0 + 5)[e + 1];
+      }
+      if (scode[e - WX] & kS) {
+        gub += P(bC0 + 1)[e - WX];
+        gvx += P(bC0 + 4)[e - WX];
+        gvy += P(bC0 + 3)[e - WX];
+      }
+      if (!(scode[e + WX] & kS)) {
+        gub -= P(bC0 + 1)[e + WX];
+        gvx -= P(bC0 + 4)[e + WX];
+        gvy -= P(bC0 + 3)[e + WX];
+      }
+      gU[j] = nU[j];
+      gUB[j] = gub;
+      gVX[j] = gvx;
+      gVY[j] = gvy;
+      gPX[j] = nPX[j];
+      gPY[j] = nPY[j];
+      gQ0[j] = nQ0[j];
+      gQ1[j] = nQ1[j];
+      gQ2[j] = nQ2[j];
+      gQ3[j] = nQ3[j];
+    }
+    __syncthreads();
+    // the later state's buffer is free: the state of step m + 2 goes there;
+    // then wait for that of step m + 1
+    if (m + 2 <= k) {
+      load_state(k - m - 2, (m + 2) % 3);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+  }
+
+  // cotangent of S_{i0} on the tile; constant cotangents added to HBM once
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    if (rx[j] < 0 || rx[j] >= TX || ry[j] < 0 || ry[j] >= TY) continue;
+    const int X = x0 + rx[j], Y = y0 + ry[j];
+    if (X >= w || Y >= h) continue;
+    const long f = (long)Y * w + X;
+    r.g_out.u[f] = gU[j];
+    r.g_out.ub[f] = gUB[j];
+    r.g_out.vbx[f] = gVX[j];
+    r.g_out.vby[f] = gVY[j];
+    r.g_out.px[f] = gPX[j];
+    r.g_out.py[f] = gPY[j];
+    r.g_out.qx[f] = gQ0[j];
+    r.g_out.qy[f] = gQ1[j];
+    r.g_out.qz[f] = gQ2[j];
+    r.g_out.qw[f] = gQ3[j];
+  }
+  for (int ci = threadIdx.x; ci < TT; ci += NT) {
+    const int cy = ci / TX, cx = ci - cy * TX;
+    const int X = x0 + cx, Y = y0 + cy;
+    if (X >= w || Y >= h) continue;
+    const long f = (long)Y * w + X;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float v = sgc[q * TT + ci];
+      if (v != 0.f) r.gc[q][f] += v;
+    }
+  }
+  block_sum_to<3>(acc, r.scal + G_LAMBDA);
+}
+
+// Blocked reverse configurations: id -> (iterations per launch, tile, threads).
+#define VFS_REVB_SHAPES(X) \
+  X(11, 2, 24, 16, 736)    \
+  X(12, 2, 16, 16, 544)    \
+  X(13, 3, 16, 16, 704)    \
+  X(14, 4, 16, 8, 640)     \
+  X(15, 2, 8, 8, 256)      \
+  X(16, 4, 8, 8, 448)
+
+cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s) {
+  switch (shape) {
+#define VFS_REVB_L(id, K, TX, TY, NT)                                                \
+  case id: {                                                                         \
+    if (r.niter > K) return cudaErrorInvalidValue;                                   \
+    dim3 grid((r.w + TX - 1) / TX, (r.h + TY - 1) / TY);                             \
+    k_rev_block<K, TX, TY, NT><<<grid, NT, RbGeom<K, TX, TY>::smem_bytes(), s>>>(r); \
+    return cudaGetLastError();                                                       \
+  }
+    VFS_REVB_SHAPES(VFS_REVB_L)
+#undef VFS_REVB_L
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int rev_block_iters(int shape) {
+  switch (shape) {
+#define VFS_REVB_K(id, K, TX, TY, NT) \
+  case id: return K;
+    VFS_REVB_SHAPES(VFS_REVB_K)
+#undef VFS_REVB_K
+    default: return 0;
+  }
+}
+
+cudaError_t prepare_rev_block() {
+  cudaError_t e = cudaSuccess;
+#define VFS_REVB_P(id, K, TX, TY, NT)                                                                 \
+  if (e == cudaSuccess)                                                                               \
+    e = cudaFuncSetAttribute(k_rev_block<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             (int)RbGeom<K, TX, TY>::smem_bytes());
+  VFS_REVB_SHAPES(VFS_REVB_P)
+#undef VFS_REVB_P
+  return e;
+}
+
 // ---------------------------------------------------------------- warp prologue reversed
 // computeDerivatives (Python/vfs.cu:120-142, 304-324) reversed: the
 // cotangents of (Iu, Iz) go to the reference level image, the warped image
@@ -1184,7 +1641,9 @@ struct VfsGradPlan {
     float* u_in;
     float* ub_in;
     float2* warp_in;
-    std::vector<TgvState> ck;  // state after iterations ckpt, 2 ckpt, ...
+    std::vector<TgvState> ck;  // state after iterations ckpt, 2 ckpt, ..., nSolverIters
+    TgvState* d_ck;            // device copy of ck (recording targets)
+    TgvState* d_seg;           // per checkpoint interval, its states (segment_lists)
   };
   std::vector<std::vector<Warp>> tape;
   float2 *tvf0 = nullptr, *cvf0 = nullptr;
@@ -1226,6 +1685,12 @@ void take_state(GCarver& cv, TgvState* s, size_t n) {
   for (auto* pp : f) *pp = cv.take<float>(n * 4);
 }
 
+// Entries of a warp's interval state lists: with ckpt 1 one list of all
+// nSolverIters + 1 states, else (ckpt + 1) per interval.
+size_t seg_entries(const VfsGradPlan* gp, const VfsParams* p) {
+  return gp->ckpt == 1 ? (size_t)p->nSolverIters + 1 : (size_t)gp->nint * (gp->ckpt + 1);
+}
+
 std::vector<std::pair<int, int>> level_sizes(const VfsParams* p) {
   std::vector<std::pair<int, int>> s;
   int h = p->height, w = p->width;
@@ -1244,7 +1709,7 @@ size_t grad_layout(VfsGradPlan* gp, const VfsParams* p, char* base) {
   const auto sz = level_sizes(p);
   const size_t n0 = (size_t)sz[0].first * sz[0].second;
   const int nW = std::max(0, p->nWarpIters);
-  const int nck = gp->nint - 1;
+  const int nck = gp->nint;
   gp->tape.assign(sz.size(), {});
   for (size_t l = 0; l < sz.size(); ++l) {
     const size_t n = (size_t)sz[l].first * sz[l].second;
@@ -1255,6 +1720,8 @@ size_t grad_layout(VfsGradPlan* gp, const VfsParams* p, char* base) {
       wt.warp_in = cv.take<float2>(n * 8);
       wt.ck.resize(std::max(0, nck));
       for (auto& s : wt.ck) take_state(cv, &s, n);
+      wt.d_ck = cv.take<TgvState>(std::max(1, nck) * sizeof(TgvState));
+      wt.d_seg = cv.take<TgvState>(seg_entries(gp, p) * sizeof(TgvState));
     }
   }
   gp->tvf0 = cv.take<float2>(n0 * 8);
@@ -1288,6 +1755,34 @@ size_t grad_layout(VfsGradPlan* gp, const VfsParams* p, char* base) {
 }
 
 int plan_bytes(const VfsParams* p, size_t* b) { return vfs_plan_workspace_size(p, b); }
+
+// The states of checkpoint interval j: its first (the warp's initial state
+// or the previous interval's last), those recomputed into the slots, and
+// its last (from the tape).
+std::vector<TgvState> interval_states(const VfsGradPlan* gp, const VfsGradPlan::Warp& wt, int j, int nI) {
+  const int nj = std::max(0, std::min(gp->ckpt, nI - j * gp->ckpt));
+  std::vector<TgvState> S(nj + 1);
+  S[0] = j == 0 ? gp->slot[0] : wt.ck[j - 1];
+  for (int q = 1; q < nj; ++q) S[q] = gp->slot[q];
+  if (nj > 0) S[nj] = wt.ck[j];
+  return S;
+}
+
+// All interval state lists of a warp, in the layout of Warp::d_seg.
+std::vector<TgvState> segment_lists(const VfsGradPlan* gp, const VfsGradPlan::Warp& wt, int nI) {
+  std::vector<TgvState> out;
+  if (gp->ckpt == 1) {
+    out.push_back(gp->slot[0]);
+    for (int i = 0; i < nI; ++i) out.push_back(wt.ck[i]);
+    return out;
+  }
+  out.resize((size_t)gp->nint * (gp->ckpt + 1));
+  for (int j = 0; j < gp->nint; ++j) {
+    const auto S = interval_states(gp, wt, j, nI);
+    std::copy(S.begin(), S.end(), out.begin() + (size_t)j * (gp->ckpt + 1));
+  }
+  return out;
+}
 
 int check_grad_params(const VfsParams* p, int ckpt) {
   std::string why;
@@ -1357,12 +1852,22 @@ int grad_forward(VfsGradPlan* gp, const float* img_ref, const float* img_other, 
       VFS_TRY(plan_warp_pre(pl, &c, s, &nk));
       TgvState cur = pl->st[0];
       int it = 0;
-      for (int j = 0; j < gp->nint; ++j) {
+      if (gp->ckpt == 1 && nI > 0) {
+        // every state recorded: the recording form of the blocked kernel
+        const int tv = tgv_has_trace(c.var) ? c.var : 134;
+        const int K = tgv_max_iters_per_launch(tv);
+        while (it < nI) {
+          const int m = std::min(K, nI - it);
+          VFS_TRY_CUDA(launch_tgv_trace(tv, cur, wt.d_ck + it, c.cst, pl->sched, it, m, pl->kc, h, w, s), "tgv");
+          cur = wt.ck[it + m - 1];
+          it += m;
+        }
+      }
+      for (int j = 0; j < gp->nint && it < nI; ++j) {
         const int end = std::min((j + 1) * gp->ckpt, nI);
         while (it < end) {
           const int m = std::min(c.K, end - it);
-          const bool ck = (it + m == end) && (j + 1 < gp->nint);
-          const TgvState out = ck ? wt.ck[j] : other_scratch(pl, cur);
+          const TgvState out = (it + m == end) ? wt.ck[j] : other_scratch(pl, cur);
           VFS_TRY_CUDA(launch_tgv_block(c.var, cur, out, c.cst, pl->sched, it, m, pl->kc, h, w, s), "tgv");
           cur = out;
           it += m;
@@ -1461,32 +1966,67 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
       VFS_TRY_CUDA(zero(gp->gcp[6], n * 4, s), "memset");
       VFS_TRY_CUDA(zero(gp->gcp[7], n * 4, s), "memset");
       int gi = 0;
-      for (int j = gp->nint - 1; j >= 0; --j) {
-        const int it0 = j * gp->ckpt;
-        const int nj = std::max(0, std::min(gp->ckpt, nI - it0));
-        std::vector<TgvState> S(nj + 1);
-        S[0] = j == 0 ? gp->slot[0] : wt.ck[j - 1];
-        for (int q = 1; q <= nj; ++q) S[q] = gp->slot[q];
-        if (tv) {
-          for (int q = 0; q < nj;) {
-            const int m = std::min(tgv_max_iters_per_launch(tv), nj - q);
-            VFS_TRY_CUDA(launch_tgv_trace(tv, S[q], gp->d_slot + q + 1, cst, pl->sched, it0 + q, m, pl->kc, h, w, s),
-                         "tgv recompute");
-            q += m;
-          }
+      // cotangent of the final state: u from the median/clamp, u_ from the
+      // next warp (or zero), v, p, q zero
+      const TgvState fin = nI > 0 ? wt.ck[gp->nint - 1] : gp->slot[0];
+      VFS_TRY_CUDA(zero_state(gp->G[gi], n, s), "memset");
+      k_g_post<<<g2d(h, w), kGB, 0, s>>>(gp->gwarp[cb], gp->gu[cb], gp->G[gi].u, fin.u, wt.u_in, pl->tvec.ptr, mask,
+                                          pl->kc.upperLimit, gp->gtvec, h, w);
+      VFS_TRY_CUDA(cudaGetLastError(), "median/clamp backward");
+      VFS_TRY_CUDA(cudaMemcpyAsync(gp->G[gi].ub, gp->gub[cb], n * 4, cudaMemcpyDeviceToDevice, s), "copy");
+      // checkpoint intervals from last to first (with ckpt 1, one interval
+      // over the whole tape)
+      const int nseg = gp->ckpt == 1 ? (nI > 0 ? 1 : 0) : gp->nint;
+      for (int j = nseg - 1; j >= 0; --j) {
+        int it0, nj;
+        std::vector<TgvState> S;
+        const TgvState* dS;
+        if (gp->ckpt == 1) {
+          it0 = 0;
+          nj = nI;
+          S = segment_lists(gp, wt, nI);
+          dS = wt.d_seg;
         } else {
-          for (int q = 1; q <= nj; ++q)
-            VFS_TRY_CUDA(launch_tgv_block(1, S[q - 1], S[q], cst, pl->sched, it0 + q - 1, 1, pl->kc, h, w, s),
-                         "tgv recompute");
+          it0 = j * gp->ckpt;
+          nj = std::max(0, std::min(gp->ckpt, nI - it0));
+          S = interval_states(gp, wt, j, nI);
+          dS = wt.d_seg + (size_t)j * (gp->ckpt + 1);
+          if (tv) {
+            for (int q = 0; q < nj - 1;) {
+              const int m = std::min(tgv_max_iters_per_launch(tv), nj - 1 - q);
+              VFS_TRY_CUDA(
+                  launch_tgv_trace(tv, S[q], gp->d_slot + q + 1, cst, pl->sched, it0 + q, m, pl->kc, h, w, s),
+                  "tgv recompute");
+              q += m;
+            }
+          } else {
+            for (int q = 1; q < nj; ++q)
+              VFS_TRY_CUDA(launch_tgv_block(1, S[q - 1], S[q], cst, pl->sched, it0 + q - 1, 1, pl->kc, h, w, s),
+                           "tgv recompute");
+          }
         }
-        if (j == gp->nint - 1) {
-          // cotangent of the final state: u from the median/clamp, u_ from
-          // the next warp (or zero), v, p, q zero
-          VFS_TRY_CUDA(zero_state(gp->G[gi], n, s), "memset");
-          k_g_post<<<g2d(h, w), kGB, 0, s>>>(gp->gwarp[cb], gp->gu[cb], gp->G[gi].u, S[nj].u, wt.u_in,
-                                              pl->tvec.ptr, mask, pl->kc.upperLimit, gp->gtvec, h, w);
-          VFS_TRY_CUDA(cudaGetLastError(), "median/clamp backward");
-          VFS_TRY_CUDA(cudaMemcpyAsync(gp->G[gi].ub, gp->gub[cb], n * 4, cudaMemcpyDeviceToDevice, s), "copy");
+        const int Kr = rev_block_iters(gp->fused_reverse);
+        if (Kr > 0) {
+          for (int i1 = nj; i1 > 0;) {
+            const int kk = std::min(Kr, i1);
+            RevBlockArgs rb;
+            rb.states = dS + (i1 - kk);
+            rb.g_in = gp->G[gi];
+            rb.g_out = gp->G[gi ^ 1];
+            rb.c = cst;
+            for (int q = 0; q < 8; ++q) rb.gc[q] = gp->gcp[q];
+            rb.sched = pl->sched;
+            rb.i0 = it0 + i1 - kk;
+            rb.niter = kk;
+            rb.k = pl->kc;
+            rb.h = h;
+            rb.w = w;
+            rb.scal = gp->scal;
+            VFS_TRY_CUDA(launch_rev_block(gp->fused_reverse, rb, s), "tgv backward");
+            gi ^= 1;
+            i1 -= kk;
+          }
+          continue;
         }
         for (int q = nj - 1; q >= 0; --q) {
           RevArgs r = rev_args(gp, cst, it0 + q, pl->kc, h, w);
@@ -1504,12 +2044,6 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
           }
           gi ^= 1;
         }
-      }
-      if (nI == 0) {
-        VFS_TRY_CUDA(zero_state(gp->G[gi], n, s), "memset");
-        k_g_post<<<g2d(h, w), kGB, 0, s>>>(gp->gwarp[cb], gp->gu[cb], gp->G[gi].u, gp->slot[0].u, wt.u_in,
-                                            pl->tvec.ptr, mask, pl->kc.upperLimit, gp->gtvec, h, w);
-        VFS_TRY_CUDA(cudaMemcpyAsync(gp->G[gi].ub, gp->gub[cb], n * 4, cudaMemcpyDeviceToDevice, s), "copy");
       }
       // derivatives, then the fetches of tvec and the warped image
       VFS_TRY_CUDA(zero(gp->gwarped, n * 4, s), "memset");
@@ -1605,6 +2139,16 @@ int vfs_grad_create(const VfsParams* prm, int ckpt_every, float f, float u0, flo
   char* gbase = reinterpret_cast<char*>(gru(reinterpret_cast<uintptr_t>(base + gru(pb, kGAlign)), kGAlign));
   grad_layout(gp, prm, gbase);
   cudaError_t e = cudaMemcpy(gp->d_slot, gp->slot.data(), gp->slot.size() * sizeof(TgvState), cudaMemcpyHostToDevice);
+  for (auto& lvl : gp->tape)
+    for (auto& wt : lvl) {
+      if (e == cudaSuccess && !wt.ck.empty())
+        e = cudaMemcpy(wt.d_ck, wt.ck.data(), wt.ck.size() * sizeof(TgvState), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) {
+        const std::vector<TgvState> seg = segment_lists(gp, wt, prm->nSolverIters);
+        e = cudaMemcpy(wt.d_seg, seg.data(), seg.size() * sizeof(TgvState), cudaMemcpyHostToDevice);
+      }
+    }
+  if (e == cudaSuccess) e = prepare_rev_block();
   if (e == cudaSuccess) e = prepare_rev_tile();
   if (e != cudaSuccess) {
     vfs_grad_destroy(gp);
@@ -1627,7 +2171,8 @@ int vfs_grad_set_options(VfsGradPlan* gp, int fused_reverse, int trace_variant) 
   if (!gp) return fail(VFS_ERR_ARG, "plan is NULL");
   if (trace_variant > 0 && !tgv_has_trace(trace_variant))
     return fail(VFS_ERR_ARG, "variant has no recording form");
-  if (fused_reverse != 0 && !rev_shape_ok(fused_reverse)) return fail(VFS_ERR_ARG, "unknown reverse tile shape");
+  if (fused_reverse != 0 && !rev_shape_ok(fused_reverse) && rev_block_iters(fused_reverse) == 0)
+    return fail(VFS_ERR_ARG, "unknown reverse kernel form");
   gp->fused_reverse = fused_reverse;
   gp->trace_variant = trace_variant;
   return VFS_OK;

@@ -62,9 +62,10 @@ class DepthSolver:
         self._recorded = None
 
     def set_options(self, fused_reverse: int = 1, trace_variant: int = 0) -> None:
-        """Backward kernel forms: the tile shape of the one-kernel reverse step
-        (1..5; 0: three gather kernels) and the TGV variant recomputing
-        checkpoint intervals (0 automatic, -1 one iteration per launch)."""
+        """Backward kernel forms (see vfs_grad_set_options in vfs_b200.h): the
+        reverse-step kernel (11..16 several iterations per launch, 1..5 one
+        tiled kernel per iteration, 0 three gather kernels) and the TGV variant
+        recomputing checkpoint intervals (0 automatic, -1 one iteration per launch)."""
         call("vfs_grad_set_options", self._gp, int(fused_reverse), int(trace_variant))
 
     def theta_of(self, param=None) -> torch.Tensor:
