@@ -152,6 +152,8 @@ def test_backward_kernel_forms_agree():
     for fused in (1, 11, 14, 16):
         s1.set_options(fused, 0)
         outs.append(_gpu_grads(s1, I0, I1, t, theta, wts))
+    s1.set_level_forms([16, 15])  # per-level forms
+    outs.append(_gpu_grads(s1, I0, I1, t, theta, wts))
     for o in outs[1:]:
         for a, b in zip(o[1:], outs[0][1:]):
             assert _rel(a, b) < 1e-5

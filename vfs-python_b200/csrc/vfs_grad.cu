@@ -1340,7 +1340,9 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   X(13, 3, 16, 16, 704)    \
   X(14, 4, 16, 8, 640)     \
   X(15, 2, 8, 8, 256)      \
-  X(16, 4, 8, 8, 448)
+  X(16, 4, 8, 8, 448)      \
+  X(17, 3, 24, 12, 768)    \
+  X(18, 2, 32, 12, 768)
 
 cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s) {
   switch (shape) {
@@ -1659,7 +1661,8 @@ struct VfsGradPlan {
   std::vector<float2*> gtvf;
   double* scal = nullptr;
   TgvState* d_slot = nullptr;  // device copy of `slot` (recording targets)
-  int fused_reverse = 1;  // reverse-step tile shape, 0: three gather kernels
+  int fused_reverse = 11;  // reverse-step kernel form (vfs_grad_set_options)
+  int level_form[32] = {0};  // per level: 0 = fused_reverse
   int trace_variant = 0;  // 0: the level's forward variant if it records, else 134
 };
 
@@ -2005,7 +2008,8 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
                            "tgv recompute");
           }
         }
-        const int Kr = rev_block_iters(gp->fused_reverse);
+        const int form = gp->level_form[l] ? gp->level_form[l] : gp->fused_reverse;
+        const int Kr = rev_block_iters(form);
         if (Kr > 0) {
           for (int i1 = nj; i1 > 0;) {
             const int kk = std::min(Kr, i1);
@@ -2022,7 +2026,7 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
             rb.h = h;
             rb.w = w;
             rb.scal = gp->scal;
-            VFS_TRY_CUDA(launch_rev_block(gp->fused_reverse, rb, s), "tgv backward");
+            VFS_TRY_CUDA(launch_rev_block(form, rb, s), "tgv backward");
             gi ^= 1;
             i1 -= kk;
           }
@@ -2034,8 +2038,8 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
           r.s1 = S[q + 1];
           r.g1 = gp->G[gi];
           r.g0 = gp->G[gi ^ 1];
-          if (gp->fused_reverse) {
-            VFS_TRY_CUDA(launch_rev_tile(gp->fused_reverse, r, s), "tgv backward");
+          if (form) {
+            VFS_TRY_CUDA(launch_rev_tile(form, r, s), "tgv backward");
           } else {
             k_rev1<<<g2d(h, w), kGB, 0, s>>>(r);
             k_rev2<<<g2d(h, w), kGB, 0, s>>>(r);
@@ -2166,6 +2170,15 @@ int vfs_grad_destroy(VfsGradPlan* gp) {
 }
 
 VfsPlan* vfs_grad_plan(VfsGradPlan* gp) { return gp ? gp->pl : nullptr; }
+
+int vfs_grad_set_level_form(VfsGradPlan* gp, int level, int form) {
+  if (!gp) return fail(VFS_ERR_ARG, "plan is NULL");
+  if (level < 0 || level >= gp->pl->L) return fail(VFS_ERR_ARG, "level out of range");
+  if (form != 0 && !rev_shape_ok(form) && rev_block_iters(form) == 0)
+    return fail(VFS_ERR_ARG, "unknown reverse kernel form");
+  gp->level_form[level] = form;
+  return VFS_OK;
+}
 
 int vfs_grad_set_options(VfsGradPlan* gp, int fused_reverse, int trace_variant) {
   if (!gp) return fail(VFS_ERR_ARG, "plan is NULL");

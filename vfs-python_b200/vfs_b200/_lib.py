@@ -121,6 +121,7 @@ _SIGS = {
     "vfs_grad_forward": [_P, _P, _P, _P, _P, _P, _P],
     "vfs_grad_backward": [_P, _P, _P, _P, _P, _P],
     "vfs_grad_set_options": [_P, _I, _I],
+    "vfs_grad_set_level_form": [_P, _I, _I],
 }
 
 _lib = None

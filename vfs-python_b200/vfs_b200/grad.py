@@ -61,12 +61,55 @@ class DepthSolver:
         self._generation = 0
         self._recorded = None
 
-    def set_options(self, fused_reverse: int = 1, trace_variant: int = 0) -> None:
+    def set_options(self, fused_reverse: int = 11, trace_variant: int = 0) -> None:
         """Backward kernel forms (see vfs_grad_set_options in vfs_b200.h): the
-        reverse-step kernel (11..16 several iterations per launch, 1..5 one
+        reverse-step kernel (11..18 several iterations per launch, 1..5 one
         tiled kernel per iteration, 0 three gather kernels) and the TGV variant
         recomputing checkpoint intervals (0 automatic, -1 one iteration per launch)."""
         call("vfs_grad_set_options", self._gp, int(fused_reverse), int(trace_variant))
+
+    def set_level_forms(self, forms) -> None:
+        """Reverse-step kernel form per level (finest first; 0 = the plan's)."""
+        for lvl, f in enumerate(forms):
+            call("vfs_grad_set_level_form", self._gp, lvl, int(f))
+        self.level_forms = list(forms)
+
+    def autotune(self, img_ref, img_other, t, theta=None, g_depth=None,
+                 forms=(11, 13, 18, 17, 12, 15, 16, 14), repeats: int = 2):
+        """Choose the reverse-step form of each level by timing whole backward
+        passes (levels are independent, so one sweep per level suffices).
+        Returns the chosen forms, finest level first."""
+        theta = self.theta_of() if theta is None else theta
+        depth = self.forward_pass(img_ref, img_other, t, theta)
+        if g_depth is None:
+            g_depth = torch.where(torch.isfinite(depth) & (self._mask != 0), torch.ones_like(depth),
+                                  torch.zeros_like(depth))
+        n_level = int(self.param.nLevel)
+        chosen = [int(forms[0])] * n_level
+        self.set_level_forms(chosen)
+
+        def timed():
+            self.backward_pass(g_depth)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(repeats):
+                self.backward_pass(g_depth)
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / repeats
+
+        for lvl in range(n_level):
+            best = None
+            for f in forms:
+                call("vfs_grad_set_level_form", self._gp, lvl, int(f))
+                ms = timed()
+                if best is None or ms < best[0]:
+                    best = (ms, int(f))
+            chosen[lvl] = best[1]
+            call("vfs_grad_set_level_form", self._gp, lvl, chosen[lvl])
+        self.level_forms = chosen
+        return chosen
 
     def theta_of(self, param=None) -> torch.Tensor:
         p = param or self.param
