@@ -345,6 +345,14 @@ def run_b200(args, n, rank, local):
         "depth_check": {"median_rel_err_vs_ground_truth": float(np.median(
             np.abs(depth[m] - pair.depth[m]) / pair.depth[m]))},
     }
+    if not args.no_fwd_bwd:
+        # the same pair through the differentiable solve (no collective: every
+        # rank measures its own)
+        fb = fwd_bwd_timing(pair, p, plain_ms=1e3 * t_max / args.steps, flush=flush)
+        fb["ms_fwd_bwd"] = max_over_ranks(fb["ms_fwd_bwd"], n)
+        fb["ratio_to_forward"] = fb["ms_fwd_bwd"] / (1e3 * t_max / args.steps)
+        fb["fwd_bwd_per_s"] = n * 1e3 / fb["ms_fwd_bwd"]
+        line["fwd_bwd"] = fb
     if n == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(pair, p, budget_s=args.cpu_budget)
     return line
@@ -478,6 +486,160 @@ def run_reference(args, n, rank, local):
     }
 
 
+def _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid):
+    """One forward + backward through DepthSolver with an L1 depth loss; returns the cotangents."""
+    depth = solver.forward_pass(ref_f, oth_f, t, theta)
+    m = valid & torch.isfinite(depth)
+    g = torch.where(m, torch.sign(depth - gt), torch.zeros_like(depth)) / m.sum().clamp(min=1)
+    return solver.backward_pass(g)
+
+
+def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None):
+    """Forward + hand-written backward of one solve through DepthSolver (L1
+    depth loss against the pair's ground truth), per-level reverse forms
+    autotuned first.  Device time with inputs resident."""
+    from vfs_b200 import DepthSolver, EquidistantCam
+    cam = EquidistantCam(pair.intrinsics)
+    solver = DepthSolver(p, cam, pair.mask, t_scale=1.0, ckpt_every=ckpt)
+    ref_f = torch.as_tensor(pair.img_ref).float().cuda()
+    oth_f = torch.as_tensor(pair.img_other).float().cuda()
+    t = torch.tensor(np.asarray(pair.t, np.float64).reshape(3))
+    theta = solver.theta_of()
+    gt = torch.as_tensor(pair.depth).cuda()
+    valid = torch.as_tensor(pair.mask != 0).cuda()
+    forms = solver.autotune(ref_f, oth_f, t, theta)
+    for _ in range(warmup):
+        _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid)
+    torch.cuda.synchronize()
+    f_ms = b_ms = 0.0
+    for _ in range(steps):
+        if flush is not None:
+            flush.zero_()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        depth = solver.forward_pass(ref_f, oth_f, t, theta)
+        e[1].record()
+        m = valid & torch.isfinite(depth)
+        g = torch.where(m, torch.sign(depth - gt), torch.zeros_like(depth)) / m.sum().clamp(min=1)
+        solver.backward_pass(g)
+        e[2].record()
+        torch.cuda.synchronize()
+        f_ms += e[0].elapsed_time(e[1])
+        b_ms += e[1].elapsed_time(e[2])
+    out = {"ms_fwd_bwd": (f_ms + b_ms) / steps, "ms_recording_forward": f_ms / steps, "ms_backward": b_ms / steps,
+           "ckpt_every": ckpt, "reverse_forms_per_level": forms, "workspace_gb": solver.workspace_bytes / 1e9}
+    if plain_ms:
+        out["ratio_to_forward"] = out["ms_fwd_bwd"] / plain_ms
+    solver.release()
+    return out
+
+
+def run_grad(args, n, rank, local):
+    """fwd+bwd solves/s: 8 pairs at 512x512, 3 levels x 5 warps x 50 iterations,
+    L1 depth loss; gradients w.r.t. both images, t and theta."""
+    from vfs_b200 import DepthSolver, EquidistantCam
+    from vfs_b200.synthetic import make_pair
+    p = params()
+    p.width = p.height = 512
+    p.nLevel, p.nWarpIters, p.nSolverIters = 3, 5, 50
+    pairs = [make_pair(512, T, seed=8 * rank + i, n_level=3) for i in range(8)]
+    cam = EquidistantCam(pairs[0].intrinsics)
+    solver = DepthSolver(p, cam, pairs[0].mask, t_scale=1.0, ckpt_every=args.ckpt)
+    dev = [(torch.as_tensor(q.img_ref).float().cuda(), torch.as_tensor(q.img_other).float().cuda(),
+            torch.tensor(np.asarray(q.t, np.float64).reshape(3)), torch.as_tensor(q.depth).cuda()) for q in pairs]
+    valid = torch.as_tensor(pairs[0].mask != 0).cuda()
+    theta = solver.theta_of()
+    forms = solver.autotune(dev[0][0], dev[0][1], dev[0][2], theta)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    # the plain forward of the same pairs (solve_stereo + triangulate_flow)
+    plains = []
+    for q in pairs:
+        vfs, cam_q = setup_b200(q, p)
+        vfs.configure(use_graph=True)
+        plains.append((vfs, cam_q, torch.as_tensor(q.img_ref).cuda(), torch.as_tensor(q.img_other).cuda(), q.t))
+
+    def plain_step():
+        for vfs, cam_q, a, b, tq in plains:
+            vfs.solve_stereo(a, b)
+            vfs.triangulate_flow(cam_q, tq)
+
+    def step():
+        for a, b, tq, gt in dev:
+            _grad_step_parts(solver, a, b, tq, theta, gt, valid)
+
+    for _ in range(args.warmup):
+        step()
+        plain_step()
+    barrier(n)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    evp = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record()
+            step()
+            ev[i][1].record()
+            flush.zero_()
+            evp[i][0].record()
+            plain_step()
+            evp[i][1].record()
+        torch.cuda.synchronize()
+    barrier(n)
+    t_grad = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1e3, n)
+    t_plain = max_over_ranks(sum(a.elapsed_time(b) for a, b in evp) / 1e3, n)
+    value = n * 8 * args.steps / t_grad
+    # end to end through the autograd API: pinned host images in, image and
+    # parameter gradients out
+    host = [(torch.as_tensor(q.img_ref).float().pin_memory(), torch.as_tensor(q.img_other).float().pin_memory())
+            for q in pairs]
+    h_out = [(torch.empty((512, 512)).pin_memory(), torch.empty((512, 512)).pin_memory(),
+              torch.empty(8, dtype=torch.float64).pin_memory()) for _ in pairs]
+
+    def e2e_step():
+        for (ha, hb), (ga_h, gb_h, gs_h), (_, _, tq, gt) in zip(host, h_out, dev):
+            a = ha.to("cuda", non_blocking=True).requires_grad_()
+            b = hb.to("cuda", non_blocking=True).requires_grad_()
+            tt = tq.clone().requires_grad_()
+            th = theta.clone().requires_grad_()
+            depth = solver(a, b, tt, th)
+            m = valid & torch.isfinite(depth.detach())
+            loss = (depth - gt).abs()[m].mean()
+            loss.backward()
+            ga_h.copy_(a.grad, non_blocking=True)
+            gb_h.copy_(b.grad, non_blocking=True)
+            gs_h[:3].copy_(tt.grad, non_blocking=True)
+            gs_h[3:].copy_(th.grad, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(n)
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(n)
+    e2e_t = max_over_ranks(e0.elapsed_time(e1) / 1e3, n)
+    return {
+        "metric": "fwd+bwd solves/s (8 pairs 512x512, 3x5x50, L1 depth loss)", "value": value, "unit": "solves/s",
+        "n_gpus": n, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_grad / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (8 seeded 512x512 fisheye pairs per rank)",
+        "config": {"workload": "8 pairs at 512x512, 3 levels x 5 warps x 50 TGV iterations, depth -> L1 loss "
+                               "against ground truth -> gradients w.r.t. both images, t, lambda, alpha0, alpha1, "
+                               "beta, gamma", "ckpt_every": args.ckpt, "reverse_forms_per_level": forms,
+                   "l2": "flushed before each step (256 MiB write outside the timed events)",
+                   "parallelism": f"dp{n} (independent pairs)"},
+        "forward_solves_per_s": n * 8 * args.steps / t_plain,
+        "ratio_fwd_bwd_to_forward": t_grad / t_plain,
+        "e2e": {"value": n * 8 * args.steps / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": 8 * 2 * 512 * 512 * 4,
+                "d2h_bytes_per_step": 8 * (2 * 512 * 512 * 4 + 64)},
+        "clocks": clk.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -487,8 +649,15 @@ def main():
     ap.add_argument("--iters-per-launch", type=int, default=134)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "batched"],
-                    help="single: the 800x800 pair (default); batched: 32 uneven pairs in one batch")
+    ap.add_argument("--workload", default="single", choices=["single", "batched", "grad"],
+                    help="single: the 800x800 pair (default); batched: 32 uneven pairs in one batch; "
+                         "grad: forward + backward of 8 pairs at 512x512")
+    ap.add_argument("--ckpt", type=int, default=1, help="grad: TGV iterations between recorded states")
+    ap.add_argument("--no-fwd-bwd", action="store_true", help="single: skip the fwd+bwd measurement")
+    ap.add_argument("--profile-grad", action="store_true",
+                    help="with --profile-case: one forward + backward at the finest level only, 1 warp, "
+                         "8 TGV iterations, every state recorded, reverse form --reverse-form")
+    ap.add_argument("--reverse-form", type=int, default=11)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--profile-case", action="store_true",
@@ -497,6 +666,25 @@ def main():
     ap.add_argument("--profile-size", type=int, default=SIZE)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 1)
+    if args.profile_case and args.profile_grad:
+        torch.cuda.set_device(0)
+        from vfs_b200 import DepthSolver, EquidistantCam
+        from vfs_b200.synthetic import make_pair
+        p = params()
+        p.width = p.height = args.profile_size
+        p.nLevel, p.nWarpIters, p.nSolverIters = 1, 1, 8
+        pair = make_pair(args.profile_size, T, seed=0, n_level=N_LEVEL)
+        solver = DepthSolver(p, EquidistantCam(pair.intrinsics), pair.mask, ckpt_every=1)
+        solver.set_options(args.reverse_form, 0)
+        gt = torch.as_tensor(pair.depth).cuda()
+        valid = torch.as_tensor(pair.mask != 0).cuda()
+        for _ in range(2):
+            _grad_step_parts(solver, torch.as_tensor(pair.img_ref).float().cuda(),
+                             torch.as_tensor(pair.img_other).float().cuda(),
+                             torch.tensor(np.asarray(pair.t, np.float64).reshape(3)), solver.theta_of(), gt, valid)
+        torch.cuda.synchronize()
+        print("profile case done")
+        return
     if args.profile_case:
         torch.cuda.set_device(0)
         p = params()
@@ -523,6 +711,10 @@ def main():
             print(json.dumps(run_reference(args, n, rank, local)), flush=True)
     elif args.workload == "batched":
         line = run_batched(args, n, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    elif args.workload == "grad":
+        line = run_grad(args, n, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)
     else:

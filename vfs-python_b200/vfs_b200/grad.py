@@ -75,16 +75,39 @@ class DepthSolver:
         self.level_forms = list(forms)
 
     def autotune(self, img_ref, img_other, t, theta=None, g_depth=None,
-                 forms=(11, 13, 18, 17, 12, 15, 16, 14), repeats: int = 2):
-        """Choose the reverse-step form of each level by timing whole backward
-        passes (levels are independent, so one sweep per level suffices).
-        Returns the chosen forms, finest level first."""
+                 forms=(11, 13, 18, 17, 12, 15, 16, 14), fwd_variants=(134, 124, 212, 216, 207),
+                 repeats: int = 2):
+        """Choose, per level, the recording forward's TGV kernel and then the
+        reverse-step form, by timing whole passes (levels are independent, so
+        one sweep per level suffices).  Returns the reverse forms, finest
+        level first; the forward choice is kept in ``level_variants``."""
         theta = self.theta_of() if theta is None else theta
+        n_level = int(self.param.nLevel)
+        # the recording forward's TGV kernel per level, among the variants that
+        # have a recording form
+        fwd_chosen = []
+        for lvl in range(n_level):
+            best = None
+            for var in fwd_variants:
+                call("vfs_plan_set_level_variant", self._plan, lvl, int(var))
+                self.forward_pass(img_ref, img_other, t, theta)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(repeats):
+                    self.forward_pass(img_ref, img_other, t, theta)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / repeats
+                if best is None or ms < best[0]:
+                    best = (ms, int(var))
+            fwd_chosen.append(best[1])
+            call("vfs_plan_set_level_variant", self._plan, lvl, best[1])
+        self.level_variants = fwd_chosen
         depth = self.forward_pass(img_ref, img_other, t, theta)
         if g_depth is None:
             g_depth = torch.where(torch.isfinite(depth) & (self._mask != 0), torch.ones_like(depth),
                                   torch.zeros_like(depth))
-        n_level = int(self.param.nLevel)
         chosen = [int(forms[0])] * n_level
         self.set_level_forms(chosen)
 
