@@ -548,7 +548,7 @@ def run_grad(args, n, rank, local):
     dev = [(torch.as_tensor(q.img_ref).float().cuda(), torch.as_tensor(q.img_other).float().cuda(),
             torch.tensor(np.asarray(q.t, np.float64).reshape(3)), torch.as_tensor(q.depth).cuda()) for q in pairs]
     valid = torch.as_tensor(pairs[0].mask != 0).cuda()
-    theta = solver.theta_of()
+    theta = solver.theta_of().clone()
     forms = solver.autotune(dev[0][0], dev[0][1], dev[0][2], theta)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     # the plain forward of the same pairs (solve_stereo + triangulate_flow)
@@ -564,8 +564,15 @@ def run_grad(args, n, rank, local):
             vfs.triangulate_flow(cam_q, tq)
 
     def step():
+        # one parameter-learning step: gradients of the 8 pairs' L1 depth
+        # losses, summed over pairs and (NCCL all-reduce) over ranks, then
+        # an SGD update of (lambda, alpha0, alpha1, beta, gamma)
+        g_theta = torch.zeros(5, dtype=torch.float64, device="cuda")
         for a, b, tq, gt in dev:
-            _grad_step_parts(solver, a, b, tq, theta, gt, valid)
+            g_theta += _grad_step_parts(solver, a, b, tq, theta, gt, valid)[3]
+        if n > 1:
+            torch.distributed.all_reduce(g_theta)
+        theta.sub_(args.lr * g_theta.cpu())
 
     for _ in range(args.warmup):
         step()
@@ -629,7 +636,9 @@ def run_grad(args, n, rank, local):
         "data": "synthetic (8 seeded 512x512 fisheye pairs per rank)",
         "config": {"workload": "8 pairs at 512x512, 3 levels x 5 warps x 50 TGV iterations, depth -> L1 loss "
                                "against ground truth -> gradients w.r.t. both images, t, lambda, alpha0, alpha1, "
-                               "beta, gamma", "ckpt_every": args.ckpt, "reverse_forms_per_level": forms,
+                               "beta, gamma; theta gradients summed over pairs and ranks, SGD step",
+                   "ckpt_every": args.ckpt, "reverse_forms_per_level": forms, "lr": args.lr,
+                   "theta_after": [float(x) for x in theta],
                    "l2": "flushed before each step (256 MiB write outside the timed events)",
                    "parallelism": f"dp{n} (independent pairs)"},
         "forward_solves_per_s": n * 8 * args.steps / t_plain,
@@ -653,6 +662,7 @@ def main():
                     help="single: the 800x800 pair (default); batched: 32 uneven pairs in one batch; "
                          "grad: forward + backward of 8 pairs at 512x512")
     ap.add_argument("--ckpt", type=int, default=1, help="grad: TGV iterations between recorded states")
+    ap.add_argument("--lr", type=float, default=1e-6, help="grad: SGD step on theta per bench step")
     ap.add_argument("--no-fwd-bwd", action="store_true", help="single: skip the fwd+bwd measurement")
     ap.add_argument("--profile-grad", action="store_true",
                     help="with --profile-case: one forward + backward at the finest level only, 1 warp, "
