@@ -488,10 +488,17 @@ def run_reference(args, n, rank, local):
     }
 
 
+def loss_mask(depth, valid):
+    """Pixels the depth loss uses: inside the mask with a plausible depth.  Near
+    the epipoles the flow carries almost no disparity and the triangulated
+    depth (and its float32 gradient, which grows as 1/disparity^2) explodes."""
+    return valid & torch.isfinite(depth) & (depth > 0) & (depth < 50)
+
+
 def _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid):
     """One forward + backward through DepthSolver with an L1 depth loss; returns the cotangents."""
     depth = solver.forward_pass(ref_f, oth_f, t, theta)
-    m = valid & torch.isfinite(depth)
+    m = loss_mask(depth, valid)
     g = torch.where(m, torch.sign(depth - gt), torch.zeros_like(depth)) / m.sum().clamp(min=1)
     return solver.backward_pass(g)
 
@@ -521,7 +528,7 @@ def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None
         e[0].record()
         depth = solver.forward_pass(ref_f, oth_f, t, theta)
         e[1].record()
-        m = valid & torch.isfinite(depth)
+        m = loss_mask(depth, valid)
         g = torch.where(m, torch.sign(depth - gt), torch.zeros_like(depth)) / m.sum().clamp(min=1)
         solver.backward_pass(g)
         e[2].record()
@@ -536,17 +543,39 @@ def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None
     return out
 
 
+GRAD_WORKLOADS = {
+    # 8 pairs at 512x512, 3 levels x 5 warps x 50 iterations, t = (0.1, 0, 0)
+    "grad": dict(size=512, n_pairs=8, levels=3, warps=5, iters=50, ckpt=10, random_t=False),
+    # parameter learning: 16 pairs at 1024x1024, 5 x 10 x 100, translation
+    # direction uniform on the sphere with magnitude in [0.05, 0.3] m
+    "learn": dict(size=1024, n_pairs=16, levels=5, warps=10, iters=100, ckpt=1, random_t=True),
+}
+
+
 def run_grad(args, n, rank, local):
-    """fwd+bwd solves/s: 8 pairs at 512x512, 3 levels x 5 warps x 50 iterations,
-    L1 depth loss; gradients w.r.t. both images, t and theta."""
+    """fwd+bwd solves/s of a parameter-learning step: per pair the L1 loss of
+    the depth map against ground truth and its gradients w.r.t. both images,
+    t and theta; theta gradients summed over pairs and ranks (NCCL), SGD step."""
     from vfs_b200 import DepthSolver, EquidistantCam
     from vfs_b200.synthetic import make_pair
+    wl = GRAD_WORKLOADS[args.workload]
+    size, n_pairs = wl["size"], wl["n_pairs"]
+    ckpt = args.ckpt if args.ckpt else wl["ckpt"]
     p = params()
-    p.width = p.height = 512
-    p.nLevel, p.nWarpIters, p.nSolverIters = 3, 5, 50
-    pairs = [make_pair(512, T, seed=8 * rank + i, n_level=3) for i in range(8)]
+    p.width = p.height = size
+    p.nLevel, p.nWarpIters, p.nSolverIters = wl["levels"], wl["warps"], wl["iters"]
+    rng = np.random.default_rng(1000 + rank)
+    pairs = []
+    for i in range(n_pairs):
+        if wl["random_t"]:
+            d = rng.standard_normal(3)
+            t_i = tuple(d / np.linalg.norm(d) * rng.uniform(0.05, 0.3))
+        else:
+            t_i = (0.1, 0.0, 0.0)
+        pairs.append(make_pair(size, t_i, seed=n_pairs * rank + i, n_level=wl["levels"]))
     cam = EquidistantCam(pairs[0].intrinsics)
-    solver = DepthSolver(p, cam, pairs[0].mask, t_scale=1.0, ckpt_every=args.ckpt)
+    torch.cuda.reset_peak_memory_stats()
+    solver = DepthSolver(p, cam, pairs[0].mask, t_scale=1.0, ckpt_every=ckpt)
     dev = [(torch.as_tensor(q.img_ref).float().cuda(), torch.as_tensor(q.img_other).float().cuda(),
             torch.tensor(np.asarray(q.t, np.float64).reshape(3)), torch.as_tensor(q.depth).cuda()) for q in pairs]
     valid = torch.as_tensor(pairs[0].mask != 0).cuda()
@@ -559,14 +588,13 @@ def run_grad(args, n, rank, local):
         vfs, cam_q = setup_b200(q, p)
         vfs.configure(use_graph=True)
         plains.append((vfs, cam_q, torch.as_tensor(q.img_ref).cuda(), torch.as_tensor(q.img_other).cuda(), q.t))
-
     def plain_step():
         for vfs, cam_q, a, b, tq in plains:
             vfs.solve_stereo(a, b)
             vfs.triangulate_flow(cam_q, tq)
 
     def step():
-        # one parameter-learning step: gradients of the 8 pairs' L1 depth
+        # one parameter-learning step: gradients of every pair's L1 depth
         # losses, summed over pairs and (NCCL all-reduce) over ranks, then
         # an SGD update of (lambda, alpha0, alpha1, beta, gamma)
         g_theta = torch.zeros(5, dtype=torch.float64, device="cuda")
@@ -574,7 +602,10 @@ def run_grad(args, n, rank, local):
             g_theta += _grad_step_parts(solver, a, b, tq, theta, gt, valid)[3]
         if n > 1:
             torch.distributed.all_reduce(g_theta)
-        theta.sub_(args.lr * g_theta.cpu())
+        # the unrolled solve's derivative can be huge (at 1024x1024, 5x10x100
+        # the theta gradients measured 1e3..1e24): clip to unit norm
+        g = g_theta.cpu()
+        theta.sub_(args.lr * g / max(1.0, float(g.norm())))
 
     for _ in range(args.warmup):
         step()
@@ -596,12 +627,12 @@ def run_grad(args, n, rank, local):
     barrier(n)
     t_grad = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1e3, n)
     t_plain = max_over_ranks(sum(a.elapsed_time(b) for a, b in evp) / 1e3, n)
-    value = n * 8 * args.steps / t_grad
+    value = n * n_pairs * args.steps / t_grad
     # end to end through the autograd API: pinned host images in, image and
     # parameter gradients out
     host = [(torch.as_tensor(q.img_ref).float().pin_memory(), torch.as_tensor(q.img_other).float().pin_memory())
             for q in pairs]
-    h_out = [(torch.empty((512, 512)).pin_memory(), torch.empty((512, 512)).pin_memory(),
+    h_out = [(torch.empty((size, size)).pin_memory(), torch.empty((size, size)).pin_memory(),
               torch.empty(8, dtype=torch.float64).pin_memory()) for _ in pairs]
 
     def e2e_step():
@@ -611,7 +642,7 @@ def run_grad(args, n, rank, local):
             tt = tq.clone().requires_grad_()
             th = theta.clone().requires_grad_()
             depth = solver(a, b, tt, th)
-            m = valid & torch.isfinite(depth.detach())
+            m = loss_mask(depth.detach(), valid)
             loss = (depth - gt).abs()[m].mean()
             loss.backward()
             ga_h.copy_(a.grad, non_blocking=True)
@@ -631,22 +662,28 @@ def run_grad(args, n, rank, local):
     torch.cuda.synchronize()
     barrier(n)
     e2e_t = max_over_ranks(e0.elapsed_time(e1) / 1e3, n)
+    desc = (f"{n_pairs} pairs at {size}x{size}, {wl['levels']} levels x {wl['warps']} warps x {wl['iters']} TGV "
+            f"iterations, " + ("translation direction uniform on the sphere, |t| in [0.05, 0.3] m" if wl["random_t"]
+                               else "t = (0.1, 0, 0) m"))
     return {
-        "metric": "fwd+bwd solves/s (8 pairs 512x512, 3x5x50, L1 depth loss)", "value": value, "unit": "solves/s",
+        "metric": f"fwd+bwd solves/s ({desc}, L1 depth loss)", "value": value, "unit": "solves/s",
         "n_gpus": n, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_grad / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (8 seeded 512x512 fisheye pairs per rank)",
-        "config": {"workload": "8 pairs at 512x512, 3 levels x 5 warps x 50 TGV iterations, depth -> L1 loss "
-                               "against ground truth -> gradients w.r.t. both images, t, lambda, alpha0, alpha1, "
-                               "beta, gamma; theta gradients summed over pairs and ranks, SGD step",
-                   "ckpt_every": args.ckpt, "reverse_forms_per_level": forms, "lr": args.lr,
+        "data": f"synthetic ({n_pairs} seeded {size}x{size} fisheye pairs per rank)",
+        "config": {"workload": desc + "; depth -> L1 loss against ground truth -> gradients w.r.t. both images, t, "
+                                      "lambda, alpha0, alpha1, beta, gamma; theta gradients summed over pairs and "
+                                      "ranks, clipped to unit norm, SGD step", "ckpt_every": ckpt, "reverse_forms_per_level": forms,
+                   "recording_forward_variants": getattr(solver, "level_variants", None), "lr": args.lr,
                    "theta_after": [float(x) for x in theta],
                    "l2": "flushed before each step (256 MiB write outside the timed events)",
                    "parallelism": f"dp{n} (independent pairs)"},
-        "forward_solves_per_s": n * 8 * args.steps / t_plain,
+        "forward_solves_per_s": n * n_pairs * args.steps / t_plain,
         "ratio_fwd_bwd_to_forward": t_grad / t_plain,
-        "e2e": {"value": n * 8 * args.steps / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": 8 * 2 * 512 * 512 * 4,
-                "d2h_bytes_per_step": 8 * (2 * 512 * 512 * 4 + 64)},
+        "workspace_gb": solver.workspace_bytes / 1e9,
+        "peak_memory_gb": torch.cuda.max_memory_allocated() / 1e9,
+        "e2e": {"value": n * n_pairs * args.steps / e2e_t, "unit": "solves/s",
+                "h2d_bytes_per_step": n_pairs * 2 * size * size * 4,
+                "d2h_bytes_per_step": n_pairs * (2 * size * size * 4 + 64)},
         "clocks": clk.summary(),
     }
 
@@ -660,11 +697,13 @@ def main():
     ap.add_argument("--iters-per-launch", type=int, default=134)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "batched", "grad"],
+    ap.add_argument("--workload", default="single", choices=["single", "batched", "grad", "learn"],
                     help="single: the 800x800 pair (default); batched: 32 uneven pairs in one batch; "
-                         "grad: forward + backward of 8 pairs at 512x512")
-    ap.add_argument("--ckpt", type=int, default=1, help="grad: TGV iterations between recorded states")
-    ap.add_argument("--lr", type=float, default=1e-6, help="grad: SGD step on theta per bench step")
+                         "grad: forward + backward of 8 pairs at 512x512; learn: 16 pairs at 1024x1024")
+    ap.add_argument("--ckpt", type=int, default=0,
+                    help="grad/learn: TGV iterations between recorded states (0: the workload's default)")
+    ap.add_argument("--lr", type=float, default=1e-3,
+                    help="grad/learn: SGD step on theta (gradient clipped to unit norm) per bench step")
     ap.add_argument("--no-fwd-bwd", action="store_true", help="single: skip the fwd+bwd measurement")
     ap.add_argument("--profile-grad", action="store_true",
                     help="with --profile-case: one forward + backward at the finest level only, 1 warp, "
@@ -725,7 +764,7 @@ def main():
         line = run_batched(args, n, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)
-    elif args.workload == "grad":
+    elif args.workload in ("grad", "learn"):
         line = run_grad(args, n, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)

@@ -157,3 +157,25 @@ def test_backward_kernel_forms_agree():
     for o in outs[1:]:
         for a, b in zip(o[1:], outs[0][1:]):
             assert _rel(a, b) < 1e-5
+
+
+def test_grad_finite_next_to_nan_flow():
+    """On this pair the forward flow is NaN at 41 pixels beside the epipole of
+    t = (0.1, 0, 0), as with the reference's own kernels (the epipolar
+    direction is undefined there).  With the depth loss restricted to
+    plausible depths the gradients stay finite: transposed fetches give
+    non-finite coordinates zero weight and are exact for any finite one."""
+    from vfs_b200 import DepthSolver, EquidistantCam
+    P = pair(512, t=(0.1, 0.0, 0.0), seed=6, n_level=3)
+    prm = bench_params(512, 512, n_level=3, n_warp=5, n_iter=30)
+    s = DepthSolver(prm, EquidistantCam(P.intrinsics), P.mask, ckpt_every=10)
+    a = torch.as_tensor(P.img_ref).float().cuda()
+    b = torch.as_tensor(P.img_other).float().cuda()
+    t = torch.tensor(P.t.reshape(3), dtype=torch.float64)
+    d = s.forward_pass(a, b, t, torch.tensor(_theta(prm)))
+    assert int(torch.isnan(d).sum()) > 0  # the case this test is about
+    gt = torch.as_tensor(P.depth).cuda()
+    m = torch.as_tensor(P.mask != 0).cuda() & torch.isfinite(d) & (d > 0) & (d < 50)
+    g = torch.where(m, torch.sign(d - gt), torch.zeros_like(d)) / m.sum()
+    for r in s.backward_pass(g):
+        assert torch.isfinite(r).all()

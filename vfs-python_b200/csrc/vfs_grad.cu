@@ -95,24 +95,38 @@ __device__ __forceinline__ void block_sum_to(const float (&v)[N], double* out) {
 struct Bilin {
   int i0, i1, j0, j1;
   float a, b;
+  bool ok;
 };
 
+// Mirror addressing has period 2n, so the texel of any finite coordinate is
+// found from floor(u) mod 2n (exact in float for integer values).  A
+// non-finite coordinate gets zero weights: no cotangent and no derivative.
+__device__ __forceinline__ void mirror_pair(float u, int n, int* i0, int* i1, float* frac) {
+  const float fu = floorf(u);
+  *frac = u - fu;
+  float r = fmodf(fu, 2.f * n);
+  if (r < 0.f) r += 2.f * n;
+  const int iu = min((int)r, 2 * n - 1);
+  *i0 = mirror_ix(iu, n);
+  *i1 = mirror_ix(iu + 1, n);
+}
+
 __device__ __forceinline__ Bilin bilin(float u, float v, int h, int w) {
-  const float fu = fminf(fmaxf(floorf(u), -1e8f), 1e8f);
-  const float fv = fminf(fmaxf(floorf(v), -1e8f), 1e8f);
   Bilin r;
-  r.a = u - fu;
-  r.b = v - fv;
-  const int iu = (int)fu, iv = (int)fv;
-  r.i0 = mirror_ix(iu, w);
-  r.i1 = mirror_ix(iu + 1, w);
-  r.j0 = mirror_ix(iv, h);
-  r.j1 = mirror_ix(iv + 1, h);
+  if (!isfinite(u) || !isfinite(v)) {
+    r.i0 = r.i1 = r.j0 = r.j1 = 0;
+    r.a = r.b = 0.f;
+    r.ok = false;
+    return r;
+  }
+  mirror_pair(u, w, &r.i0, &r.i1, &r.a);
+  mirror_pair(v, h, &r.j0, &r.j1, &r.b);
+  r.ok = true;
   return r;
 }
 
 __device__ __forceinline__ void scatter1(float* g, int w, const Bilin& B, float val) {
-  if (val == 0.f) return;
+  if (val == 0.f || !B.ok) return;
   atomicAdd(g + (long)B.j0 * w + B.i0, (1.f - B.a) * (1.f - B.b) * val);
   atomicAdd(g + (long)B.j0 * w + B.i1, B.a * (1.f - B.b) * val);
   atomicAdd(g + (long)B.j1 * w + B.i0, (1.f - B.a) * B.b * val);
@@ -120,6 +134,7 @@ __device__ __forceinline__ void scatter1(float* g, int w, const Bilin& B, float 
 }
 
 __device__ __forceinline__ void scatter2(float2* g, int w, const Bilin& B, float2 val) {
+  if (!B.ok) return;
   float* f = reinterpret_cast<float*>(g);
   const float wt[4] = {(1.f - B.a) * (1.f - B.b), B.a * (1.f - B.b), (1.f - B.a) * B.b, B.a * B.b};
   const long ix[4] = {(long)B.j0 * w + B.i0, (long)B.j0 * w + B.i1, (long)B.j1 * w + B.i0, (long)B.j1 * w + B.i1};
@@ -132,12 +147,14 @@ __device__ __forceinline__ void scatter2(float2* g, int w, const Bilin& B, float
 
 // d(fetch)/du, d(fetch)/dv of a one-channel plane.
 __device__ __forceinline__ float2 bilin_d1(Plane<const float> T, const Bilin& B) {
+  if (!B.ok) return make_float2(0.f, 0.f);
   const float t00 = T.at(B.i0, B.j0), t01 = T.at(B.i1, B.j0), t10 = T.at(B.i0, B.j1), t11 = T.at(B.i1, B.j1);
   return make_float2((1.f - B.b) * (t01 - t00) + B.b * (t11 - t10), (1.f - B.a) * (t10 - t00) + B.a * (t11 - t01));
 }
 
 // g . d(fetch)/du, g . d(fetch)/dv of a two-channel plane.
 __device__ __forceinline__ float2 bilin_d2(Plane<const float2> T, const Bilin& B, float2 g) {
+  if (!B.ok) return make_float2(0.f, 0.f);
   const float2 t00 = T.at(B.i0, B.j0), t01 = T.at(B.i1, B.j0), t10 = T.at(B.i0, B.j1), t11 = T.at(B.i1, B.j1);
   const float dux = (1.f - B.b) * (t01.x - t00.x) + B.b * (t11.x - t10.x);
   const float duy = (1.f - B.b) * (t01.y - t00.y) + B.b * (t11.y - t10.y);
@@ -1244,6 +1261,9 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       for (int q = 0; q < 6; ++q) P(bC0 + q)[e] = Cv[q];
     }
     __syncthreads();
+    // the later state's buffer is no longer read: the state of step m + 2
+    // starts loading into it while phase 3 runs
+    if (m + 2 <= k) load_state(k - m - 2, (m + 2) % 3);
     // phase 3: transposed gradients of u_ and v_ on [lo, hi); commit the step
 #pragma unroll
     for (int j = 0; j < J; ++j) {
@@ -1289,11 +1309,8 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       gQ2[j] = nQ2[j];
       gQ3[j] = nQ3[j];
     }
-    __syncthreads();
-    // the later state's buffer is free: the state of step m + 2 goes there;
-    // then wait for that of step m + 1
+    // wait for the state of step m + 1
     if (m + 2 <= k) {
-      load_state(k - m - 2, (m + 2) % 3);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();

@@ -105,9 +105,9 @@ class DepthSolver:
             call("vfs_plan_set_level_variant", self._plan, lvl, best[1])
         self.level_variants = fwd_chosen
         depth = self.forward_pass(img_ref, img_other, t, theta)
-        if g_depth is None:
-            g_depth = torch.where(torch.isfinite(depth) & (self._mask != 0), torch.ones_like(depth),
-                                  torch.zeros_like(depth))
+        if g_depth is None:  # unit cotangent where the depth is finite and not near-singular
+            g_depth = torch.where(torch.isfinite(depth) & (depth.abs() < 1e3) & (self._mask != 0),
+                                  torch.ones_like(depth), torch.zeros_like(depth))
         chosen = [int(forms[0])] * n_level
         self.set_level_forms(chosen)
 
