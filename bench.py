@@ -235,8 +235,8 @@ def cpu_baseline_sample(pair, p, budget_s=20.0):
                       f"iterations ({t_map:.0f} s per map)"}
 
 
-def load_traffic():
-    path = os.path.join(ROOT, "profiles", "k_tgv_reg_800x800_ncu.json")
+def load_traffic(name="k_tgv_reg_800x800_ncu.json"):
+    path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as f:
             return json.load(f)
@@ -503,6 +503,24 @@ def _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid):
     return solver.backward_pass(g)
 
 
+def reverse_roofline(solver, run_once):
+    """Live roofline of the reverse TGV launches: one extra forward + backward
+    with event timing around the reverse launches (outside any timed loop)."""
+    tr = load_traffic("k_rev_block_800x800_ncu.json")
+    solver.set_timing(True)
+    run_once()
+    st = solver.backward_stats()
+    solver.set_timing(False)
+    peak, kind = measured_peak()
+    achieved = st["tgv_alg_bytes"] / (st["tgv_ms"] / 1e3) / 1e9 if st["tgv_ms"] > 0 else None
+    return {"bound": "hbm", "kernel": "k_rev_block (reverse TGV iterations)", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": kind,
+            "alg_bytes_per_pixel_iteration": 241, "alg_bytes_per_launch": st["tgv_alg_bytes"] / max(st["tgv_launches"], 1),
+            "avg_launch_us": 1e3 * st["tgv_ms"] / max(st["tgv_launches"], 1), "reverse_tgv_ms": st["tgv_ms"],
+            "reverse_tgv_ms_per_level": st["tgv_ms_level"],
+            "traffic": (tr["dram_bytes_per_alg_byte"] * st["tgv_alg_bytes"] / max(st["tgv_launches"], 1)) if tr else None}
+
+
 def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None):
     """Forward + hand-written backward of one solve through DepthSolver (L1
     depth loss against the pair's ground truth), per-level reverse forms
@@ -536,7 +554,8 @@ def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None
         f_ms += e[0].elapsed_time(e[1])
         b_ms += e[1].elapsed_time(e[2])
     out = {"ms_fwd_bwd": (f_ms + b_ms) / steps, "ms_recording_forward": f_ms / steps, "ms_backward": b_ms / steps,
-           "ckpt_every": ckpt, "reverse_forms_per_level": forms, "workspace_gb": solver.workspace_bytes / 1e9}
+           "ckpt_every": ckpt, "reverse_forms_per_level": forms, "workspace_gb": solver.workspace_bytes / 1e9,
+           "roofline": reverse_roofline(solver, lambda: _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid))}
     if plain_ms:
         out["ratio_to_forward"] = out["ms_fwd_bwd"] / plain_ms
     solver.release()
@@ -662,6 +681,8 @@ def run_grad(args, n, rank, local):
     torch.cuda.synchronize()
     barrier(n)
     e2e_t = max_over_ranks(e0.elapsed_time(e1) / 1e3, n)
+    a0, b0, t0_, gt0 = dev[0]
+    roof = reverse_roofline(solver, lambda: _grad_step_parts(solver, a0, b0, t0_, theta, gt0, valid))
     desc = (f"{n_pairs} pairs at {size}x{size}, {wl['levels']} levels x {wl['warps']} warps x {wl['iters']} TGV "
             f"iterations, " + ("translation direction uniform on the sphere, |t| in [0.05, 0.3] m" if wl["random_t"]
                                else "t = (0.1, 0, 0) m"))
@@ -681,6 +702,7 @@ def run_grad(args, n, rank, local):
         "ratio_fwd_bwd_to_forward": t_grad / t_plain,
         "workspace_gb": solver.workspace_bytes / 1e9,
         "peak_memory_gb": torch.cuda.max_memory_allocated() / 1e9,
+        "roofline": roof,
         "e2e": {"value": n * n_pairs * args.steps / e2e_t, "unit": "solves/s",
                 "h2d_bytes_per_step": n_pairs * 2 * size * size * 4,
                 "d2h_bytes_per_step": n_pairs * (2 * size * size * 4 + 64)},

@@ -273,6 +273,14 @@ VFS_API int vfs_grad_set_options(VfsGradPlan* plan, int fused_reverse, int trace
 /* Reverse-step kernel form for one level (0: the plan's, from
  * vfs_grad_set_options; default 11).  Level 0 is the finest. */
 VFS_API int vfs_grad_set_level_form(VfsGradPlan* plan, int level, int form);
+/* Event timing of the reverse TGV launches of each backward (off by default).
+ * vfs_grad_stats (after synchronising) fills tgv_ms, tgv_alg_bytes (241 per
+ * pixel and reversed iteration: state before 40, p and q after 24, cotangent
+ * in 40 and out 40, constants 33, constant cotangents read and written 64),
+ * tgv_launches, tgv_intervals and tgv_ms_level for the last backward;
+ * kernels_per_solve is 0. */
+VFS_API int vfs_grad_set_timing(VfsGradPlan* plan, int enable);
+VFS_API int vfs_grad_stats(VfsGradPlan* plan, VfsSolveStats* out);
 
 #ifdef __cplusplus
 }

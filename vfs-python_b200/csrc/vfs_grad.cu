@@ -1679,6 +1679,13 @@ struct VfsGradPlan {
   double* scal = nullptr;
   TgvState* d_slot = nullptr;  // device copy of `slot` (recording targets)
   int fused_reverse = 11;  // reverse-step kernel form (vfs_grad_set_options)
+  // instrumentation: an event pair around each interval's reverse launches
+  bool timing = false;
+  std::vector<cudaEvent_t> tev;
+  std::vector<double> tev_bytes;
+  std::vector<long long> tev_launches;
+  std::vector<int> tev_level;
+  int tev_used = 0;
   int level_form[32] = {0};  // per level: 0 = fused_reverse
   int trace_variant = 0;  // 0: the level's forward variant if it records, else 134
 };
@@ -1938,6 +1945,7 @@ cudaError_t zero_state(const TgvState& st, size_t n, cudaStream_t s) {
 int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_other, double* g_scalars,
                   cudaStream_t s) {
   VfsPlan* pl = gp->pl;
+  gp->tev_used = 0;
   const int L = pl->L, nW = pl->prm.nWarpIters, nI = pl->prm.nSolverIters;
   const auto& v0 = pl->lv[0];
   const size_t n0 = (size_t)v0.h * v0.w;
@@ -2027,6 +2035,26 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
         }
         const int form = gp->level_form[l] ? gp->level_form[l] : gp->fused_reverse;
         const int Kr = rev_block_iters(form);
+        int pair = -1;
+        if (gp->timing && nj > 0) {
+          pair = gp->tev_used++;
+          while ((int)gp->tev.size() < 2 * (pair + 1)) {
+            cudaEvent_t e;
+            VFS_TRY_CUDA(cudaEventCreate(&e), "event create");
+            gp->tev.push_back(e);
+          }
+          gp->tev_bytes.resize(pair + 1);
+          gp->tev_launches.resize(pair + 1);
+          gp->tev_level.resize(pair + 1);
+          // algorithmic bytes of one reversed iteration, per pixel: the state
+          // before (40) and the p, q after it (24), the cotangent in (40) and
+          // out (40), the constants (33), the constant cotangents read and
+          // written (64)
+          gp->tev_bytes[pair] = 241.0 * (double)n * nj;
+          gp->tev_launches[pair] = Kr > 0 ? (nj + Kr - 1) / Kr : (form ? nj : 3 * nj);
+          gp->tev_level[pair] = l;
+          VFS_TRY_CUDA(cudaEventRecord(gp->tev[2 * pair], s), "event record");
+        }
         if (Kr > 0) {
           for (int i1 = nj; i1 > 0;) {
             const int kk = std::min(Kr, i1);
@@ -2047,6 +2075,7 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
             gi ^= 1;
             i1 -= kk;
           }
+          if (pair >= 0) VFS_TRY_CUDA(cudaEventRecord(gp->tev[2 * pair + 1], s), "event record");
           continue;
         }
         for (int q = nj - 1; q >= 0; --q) {
@@ -2065,6 +2094,7 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
           }
           gi ^= 1;
         }
+        if (pair >= 0) VFS_TRY_CUDA(cudaEventRecord(gp->tev[2 * pair + 1], s), "event record");
       }
       // derivatives, then the fetches of tvec and the warped image
       VFS_TRY_CUDA(zero(gp->gwarped, n * 4, s), "memset");
@@ -2181,12 +2211,36 @@ int vfs_grad_create(const VfsParams* prm, int ckpt_every, float f, float u0, flo
 
 int vfs_grad_destroy(VfsGradPlan* gp) {
   if (!gp) return VFS_OK;
+  for (auto e : gp->tev) cudaEventDestroy(e);
   vfs_plan_destroy(gp->pl);
   delete gp;
   return VFS_OK;
 }
 
 VfsPlan* vfs_grad_plan(VfsGradPlan* gp) { return gp ? gp->pl : nullptr; }
+
+int vfs_grad_set_timing(VfsGradPlan* gp, int enable) {
+  if (!gp) return fail(VFS_ERR_ARG, "plan is NULL");
+  gp->timing = enable != 0;
+  return VFS_OK;
+}
+
+int vfs_grad_stats(VfsGradPlan* gp, VfsSolveStats* out) {
+  if (!gp || !out) return fail(VFS_ERR_ARG, "NULL argument");
+  memset(out, 0, sizeof(*out));
+  if (!gp->timing) return VFS_OK;
+  for (int i = 0; i < gp->tev_used; ++i) {
+    float t = 0;
+    VFS_TRY_CUDA(cudaEventElapsedTime(&t, gp->tev[2 * i], gp->tev[2 * i + 1]), "event elapsed (synchronise first)");
+    out->tgv_ms += t;
+    out->tgv_alg_bytes += gp->tev_bytes[i];
+    out->tgv_launches += gp->tev_launches[i];
+    const int lvl = gp->tev_level[i];
+    if (lvl >= 0 && lvl < 16) out->tgv_ms_level[lvl] += t;
+  }
+  out->tgv_intervals = gp->tev_used;
+  return VFS_OK;
+}
 
 int vfs_grad_set_level_form(VfsGradPlan* gp, int level, int form) {
   if (!gp) return fail(VFS_ERR_ARG, "plan is NULL");

@@ -134,6 +134,17 @@ class DepthSolver:
         self.level_forms = chosen
         return chosen
 
+    def set_timing(self, enable: bool) -> None:
+        call("vfs_grad_set_timing", self._gp, int(bool(enable)))
+
+    def backward_stats(self) -> dict:
+        """Timing of the last backward's reverse TGV launches (set_timing(True) first)."""
+        torch.cuda.current_stream().synchronize()
+        st = _lib.VfsSolveStats()
+        call("vfs_grad_stats", self._gp, ctypes.byref(st))
+        return {"tgv_ms": st.tgv_ms, "tgv_alg_bytes": st.tgv_alg_bytes, "tgv_launches": st.tgv_launches,
+                "tgv_ms_level": list(st.tgv_ms_level)[: int(self.param.nLevel)]}
+
     def theta_of(self, param=None) -> torch.Tensor:
         p = param or self.param
         return torch.tensor([float(getattr(p, k)) for k in THETA], dtype=torch.float64)
