@@ -970,10 +970,16 @@ enum { sUB, sVX, sVY, sU, sPX, sPY, sQX, sQY, sQZ, sQW, kStPlanes };
 enum RbPlane { bS0 = 0, bAX = 3 * kStPlanes, bAY, bAB, bC0, bCA = bC0 + 6, bCB, bCC, bREX, bREY, bREZ, bIU, bIZ,
                kRbPlanes };
 
+// The window starts LHX >= K+1 columns left of the tile, rounded to a
+// multiple of 4, and is a multiple of 4 wide: with a row stride divisible by
+// 4 every window row then starts on a 16-byte boundary and the recorded
+// states load as 16-byte chunks.
 template <int K, int TX, int TY>
 struct RbGeom {
+  static_assert(TX % 4 == 0, "tile width must be a multiple of 4");
   static constexpr int LH = K + 1;
-  static constexpr int WX = TX + 3 * K + 1, WY = TY + 3 * K + 1, N = WX * WY;
+  static constexpr int LHX = (K + 1 + 3) / 4 * 4;
+  static constexpr int WX = (TX + LHX + 2 * K + 3) / 4 * 4, WY = TY + 3 * K + 1, N = WX * WY;
   static constexpr size_t smem_bytes() {
     return (size_t)kRbPlanes * N * 4 + (size_t)8 * TX * TY * 4 + ((N + 15) / 16) * 16;
   }
@@ -983,6 +989,10 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool ok)
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 4 : 0) : "memory");
 }
+__device__ __forceinline__ void cp_async16(float* dst, const float* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 16 : 0) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int NG>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NG) : "memory"); }
@@ -990,7 +1000,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <int K, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   using G = RbGeom<K, TX, TY>;
-  constexpr int WX = G::WX, N = G::N, LH = G::LH, J = (N + NT - 1) / NT, TT = TX * TY;
+  static_assert(G::N <= NT, "one window pixel per thread");
+  constexpr int WX = G::WX, N = G::N, LH = G::LH, LHX = G::LHX, J = (N + NT - 1) / NT, TT = TX * TY;
   extern __shared__ float4 smem_raw[];
   float* const sm = reinterpret_cast<float*>(smem_raw);
   float* const sgc = sm + (size_t)kRbPlanes * N;
@@ -999,7 +1010,8 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   const int w = r.w, h = r.h;
   const long n = (long)h * w;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const long base = (long)(y0 - LH) * w + (x0 - LH);
+  const long base = (long)(y0 - LH) * w + (x0 - LHX);
+  const bool vec4 = (w % 4) == 0;
   const int k = r.niter < K ? r.niter : K;
   const float eps = 1E-7f;
   const float al0 = r.k.alpha0, al1 = r.k.alpha1, lam = r.k.lambda;
@@ -1016,14 +1028,31 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     const int m = k - q;
     const int lo = m == 0 ? -LH : -(k - m) - 2, hiX = m == 0 ? TX + 2 * K : TX + 2 * (k - m) + 2,
               hiY = m == 0 ? TY + 2 * K : TY + 2 * (k - m) + 2;
+    if (vec4) {
+      // 16-byte chunks along rows (a chunk is wholly inside or outside
+      // [0, n) since n and the chunk start are multiples of 4)
+      for (int c = threadIdx.x; c < N / 4; c += NT) {
+        const int e0 = 4 * c;
+        const int wy = e0 / WX, wx0 = e0 - wy * WX;
+        const int cx = wx0 - LHX, cy = wy - LH;
+        if (cy < lo || cy >= hiY || cx + 3 < lo || cx >= hiX) continue;
+        const long f = base + (long)wy * w + wx0;
+        const bool ok = f >= 0 && f < n;
 #pragma unroll
-    for (int j = 0; j < J; ++j) {
-      if (rx[j] < lo || rx[j] >= hiX || ry[j] < lo || ry[j] >= hiY) continue;
-      const int e = threadIdx.x + j * NT;
-      const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LH);
-      const bool ok = f >= 0 && f < n;
+        for (int pl = 0; pl < kStPlanes; ++pl)
+          cp_async16(P(bS0 + b * kStPlanes + pl) + e0, ok ? src[pl] + f : src[pl], ok);
+      }
+    } else {
 #pragma unroll
-      for (int pl = 0; pl < kStPlanes; ++pl) cp_async4(P(bS0 + b * kStPlanes + pl) + e, ok ? src[pl] + f : src[pl], ok);
+      for (int j = 0; j < J; ++j) {
+        if (rx[j] < lo || rx[j] >= hiX || ry[j] < lo || ry[j] >= hiY) continue;
+        const int e = threadIdx.x + j * NT;
+        const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LHX);
+        const bool ok = f >= 0 && f < n;
+#pragma unroll
+        for (int pl = 0; pl < kStPlanes; ++pl)
+          cp_async4(P(bS0 + b * kStPlanes + pl) + e, ok ? src[pl] + f : src[pl], ok);
+      }
     }
     cp_async_commit();
   };
@@ -1032,7 +1061,7 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   for (int j = 0; j < J; ++j) {
     const int e = threadIdx.x + j * NT;
     const int wy = e / WX, wx = e - wy * WX;
-    rx[j] = wx - LH;
+    rx[j] = wx - LHX;
     ry[j] = e < N ? wy - LH : (1 << 20);
   }
   load_state(k, 0);
@@ -1041,7 +1070,7 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int e = threadIdx.x + j * NT;
-    const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LH);
+    const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LHX);
     const bool ok = e < N && f >= 0 && f < n;
     gU[j] = ok ? r.g_in.u[f] : 0.f;
     gUB[j] = ok ? r.g_in.ub[f] : 0.f;
@@ -1082,7 +1111,7 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       nU[j] = lUB[j] = lVX[j] = lVY[j] = 0.f;
       if (rx[j] < lo - 1 || rx[j] >= hiX + 2 || ry[j] < lo - 1 || ry[j] >= hiY + 2) continue;
       const int e = threadIdx.x + j * NT;
-      const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LH);
+      const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LHX);
       const uint8_t c = scode[e];
       const bool core = rx[j] >= 0 && rx[j] < TX && ry[j] >= 0 && ry[j] < TY && x0 + rx[j] < w && y0 + ry[j] < h;
       float Ax = 0.f, Ay = 0.f, Bv = 0.f;
@@ -1168,7 +1197,7 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       nPX[j] = nPY[j] = nQ0[j] = nQ1[j] = nQ2[j] = nQ3[j] = 0.f;
       if (rx[j] < lo - 1 || rx[j] >= hiX + 1 || ry[j] < lo - 1 || ry[j] >= hiY + 1) continue;
       const int e = threadIdx.x + j * NT;
-      const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LH);
+      const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LHX);
       const uint8_t c = scode[e];
       const bool core = rx[j] >= 0 && rx[j] < TX && ry[j] >= 0 && ry[j] < TY && x0 + rx[j] < w && y0 + ry[j] < h;
       float Cv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1353,12 +1382,12 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 // Blocked reverse configurations: id -> (iterations per launch, tile, threads).
 #define VFS_REVB_SHAPES(X) \
   X(11, 2, 24, 16, 736)    \
-  X(12, 2, 16, 16, 544)    \
-  X(13, 3, 16, 16, 704)    \
-  X(14, 4, 16, 8, 640)     \
+  X(12, 2, 16, 16, 576)    \
+  X(13, 3, 16, 16, 736)    \
+  X(14, 4, 16, 8, 672)     \
   X(15, 2, 8, 8, 256)      \
-  X(16, 4, 8, 8, 448)      \
-  X(17, 3, 24, 12, 768)    \
+  X(16, 4, 8, 8, 512)      \
+  X(17, 3, 24, 12, 800)    \
   X(18, 2, 32, 12, 768)
 
 cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s) {
