@@ -1067,6 +1067,29 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   load_state(k, 0);
   if (k >= 1) load_state(k - 1, 1);
   if (k >= 2) load_state(k - 2, 2);
+  // a launch that follows another reverse launch may start before it ends:
+  // everything above and the constants below are recorded data; the
+  // cotangent it wrote is read only after griddepcontrol.wait
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int e = threadIdx.x + j * NT;
+    const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LHX);
+    const bool ok = e < N && f >= 0 && f < n;
+    if (e < N) {
+      P(bCA)[e] = ok ? r.c.a[f] : 0.f;
+      P(bCB)[e] = ok ? r.c.b[f] : 0.f;
+      P(bCC)[e] = ok ? r.c.c[f] : 0.f;
+      const float ex = ok ? r.c.ex[f] : 0.f, ey = ok ? r.c.ey[f] : 0.f, ez = ok ? r.c.ez[f] : 0.f;
+      P(bREX)[e] = fabsf(ex) < eps ? 0.f : 1.f / ex;
+      P(bREY)[e] = fabsf(ey) < eps ? 0.f : 1.f / ey;
+      P(bREZ)[e] = fabsf(ez) < eps ? 0.f : 1.f / ez;
+      P(bIU)[e] = ok ? r.c.iu[f] : 0.f;
+      P(bIZ)[e] = ok ? r.c.iz[f] : 0.f;
+      scode[e] = ok ? r.c.code[f] : 0;
+    }
+  }
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int e = threadIdx.x + j * NT;
@@ -1082,18 +1105,6 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     gQ1[j] = ok ? r.g_in.qy[f] : 0.f;
     gQ2[j] = ok ? r.g_in.qz[f] : 0.f;
     gQ3[j] = ok ? r.g_in.qw[f] : 0.f;
-    if (e < N) {
-      P(bCA)[e] = ok ? r.c.a[f] : 0.f;
-      P(bCB)[e] = ok ? r.c.b[f] : 0.f;
-      P(bCC)[e] = ok ? r.c.c[f] : 0.f;
-      const float ex = ok ? r.c.ex[f] : 0.f, ey = ok ? r.c.ey[f] : 0.f, ez = ok ? r.c.ez[f] : 0.f;
-      P(bREX)[e] = fabsf(ex) < eps ? 0.f : 1.f / ex;
-      P(bREY)[e] = fabsf(ey) < eps ? 0.f : 1.f / ey;
-      P(bREZ)[e] = fabsf(ez) < eps ? 0.f : 1.f / ez;
-      P(bIU)[e] = ok ? r.c.iu[f] : 0.f;
-      P(bIZ)[e] = ok ? r.c.iz[f] : 0.f;
-      scode[e] = ok ? r.c.code[f] : 0;
-    }
   }
   for (int q = threadIdx.x; q < 8 * TT; q += NT) sgc[q] = 0.f;
   if (k >= 2) cp_async_wait<1>(); else cp_async_wait<0>();
@@ -1392,12 +1403,20 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 
 cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s) {
   switch (shape) {
-#define VFS_REVB_L(id, K, TX, TY, NT)                                                \
-  case id: {                                                                         \
-    if (r.niter > K) return cudaErrorInvalidValue;                                   \
-    dim3 grid((r.w + TX - 1) / TX, (r.h + TY - 1) / TY);                             \
-    k_rev_block<K, TX, TY, NT><<<grid, NT, RbGeom<K, TX, TY>::smem_bytes(), s>>>(r); \
-    return cudaGetLastError();                                                       \
+#define VFS_REVB_L(ID, K, TX, TY, NT)                                              \
+  case ID: {                                                                       \
+    if (r.niter > K) return cudaErrorInvalidValue;                                 \
+    cudaLaunchConfig_t cfg = {};                                                   \
+    cfg.gridDim = dim3((r.w + TX - 1) / TX, (r.h + TY - 1) / TY);                  \
+    cfg.blockDim = dim3(NT);                                                       \
+    cfg.dynamicSmemBytes = RbGeom<K, TX, TY>::smem_bytes();                        \
+    cfg.stream = s;                                                                \
+    cudaLaunchAttribute at[1];                                                     \
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                 \
+    at[0].val.programmaticStreamSerializationAllowed = 1;                          \
+    cfg.attrs = at;                                                                \
+    cfg.numAttrs = 1;                                                              \
+    return cudaLaunchKernelEx(&cfg, k_rev_block<K, TX, TY, NT>, r);                \
   }
     VFS_REVB_SHAPES(VFS_REVB_L)
 #undef VFS_REVB_L
