@@ -1401,7 +1401,10 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   X(17, 3, 24, 12, 800)    \
   X(18, 2, 32, 12, 768)
 
-cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s) {
+// pdl: may start as a programmatic dependent of the previous launch (only
+// when that launch wrote none of the recorded states this one reads before
+// its griddepcontrol.wait, i.e. not right after a recomputation).
+cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s, bool pdl) {
   switch (shape) {
 #define VFS_REVB_L(ID, K, TX, TY, NT)                                              \
   case ID: {                                                                       \
@@ -1415,7 +1418,7 @@ cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s) {
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                 \
     at[0].val.programmaticStreamSerializationAllowed = 1;                          \
     cfg.attrs = at;                                                                \
-    cfg.numAttrs = 1;                                                              \
+    cfg.numAttrs = pdl ? 1 : 0;                                                    \
     return cudaLaunchKernelEx(&cfg, k_rev_block<K, TX, TY, NT>, r);                \
   }
     VFS_REVB_SHAPES(VFS_REVB_L)
@@ -2119,7 +2122,8 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
             rb.h = h;
             rb.w = w;
             rb.scal = gp->scal;
-            VFS_TRY_CUDA(launch_rev_block(form, rb, s), "tgv backward");
+            // right after a recomputation the states were just written
+            VFS_TRY_CUDA(launch_rev_block(form, rb, s, !(gp->ckpt > 1 && i1 == nj)), "tgv backward");
             gi ^= 1;
             i1 -= kk;
           }

@@ -230,13 +230,30 @@ cudaError_t batch_block(const TgvBatchItem*, int, int, int, const float3*, int, 
   return cudaErrorInvalidValue;  // batched launches use the register-owned kernels
 }
 
+// A launch configuration that lets the kernel start as a programmatic
+// dependent of the previous launch on the stream (the kernels wait for it
+// with griddepcontrol.wait before reading what it wrote).
+struct PdlLaunch {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  PdlLaunch(dim3 grid, int threads, size_t smem, cudaStream_t s) {
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+  }
+};
+
 template <int K, int TX, int TY, int NT>
 cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts& c, const float3* sched, int it0,
                        int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
   dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);
-  k_tgv_reg<K, TX, TY, NT><<<grid, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(in, out, c, sched, it0, niter, kc, h,
-                                                                               w);
-  cudaError_t e = cudaGetLastError();
+  PdlLaunch L(grid, NT, RegGeom<K, TX, TY>::smem_bytes(), s);
+  cudaError_t e = cudaLaunchKernelEx(&L.cfg, k_tgv_reg<K, TX, TY, NT>, in, out, c, sched, it0, niter, kc, h, w);
   if (e != cudaSuccess) {
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, k_tgv_reg<K, TX, TY, NT>);
@@ -334,10 +351,9 @@ cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState* tr
 #define VFS_LAUNCH_T(id, K, TX, TY, NT)                                                                    \
   case id: {                                                                                               \
     if (niter > K) return cudaErrorInvalidValue;                                                           \
-    dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);                                                       \
-    k_tgv_reg_trace<K, TX, TY, NT><<<grid, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(in, trace, c, sched, it0, \
-                                                                                       niter, kc, h, w);   \
-    return cudaGetLastError();                                                                             \
+    PdlLaunch L(dim3((w + TX - 1) / TX, (h + TY - 1) / TY), NT, RegGeom<K, TX, TY>::smem_bytes(), s);     \
+    return cudaLaunchKernelEx(&L.cfg, k_tgv_reg_trace<K, TX, TY, NT>, in, trace, c, sched, it0, niter, kc, h, \
+                              w);                                                                          \
   }
     VFS_TGV_TRACE_VARIANTS(VFS_LAUNCH_T)
 #undef VFS_LAUNCH_T

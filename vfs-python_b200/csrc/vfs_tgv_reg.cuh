@@ -52,6 +52,11 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   float ru[J], rpx[J], rpy[J], ra[J], rb[J], rc[J], rex[J], rey[J], rez[J], riu[J], riz[J];
   int rcode[J], rwx[J], rwy[J];
 
+  // When launched as a programmatic dependent of the previous TGV launch this
+  // CTA may start before that launch ends: the per-warp constants are read
+  // first, the state (which that launch writes) only after griddepcontrol.wait
+  // (a no-op for an ordinary launch).
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int e = threadIdx.x + j * NT;
@@ -60,9 +65,6 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     rwy[j] = e < N ? wy : 1 << 20;  // never inside a region
     const long f = base + (long)wy * w + wx;
     const bool ok = e < N && f >= 0 && f < n;
-    ru[j] = ok ? in.u[f] : 0.f;
-    rpx[j] = ok ? in.px[f] : 0.f;
-    rpy[j] = ok ? in.py[f] : 0.f;
     ra[j] = ok ? cst.a[f] : 0.f;
     rb[j] = ok ? cst.b[f] : 0.f;
     rc[j] = ok ? cst.c[f] : 0.f;
@@ -72,6 +74,16 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     riu[j] = ok ? cst.iu[f] : 0.f;
     riz[j] = ok ? cst.iz[f] : 0.f;
     rcode[j] = ok ? cst.code[f] : 0;
+  }
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int e = threadIdx.x + j * NT;
+    const long f = base + (long)rwy[j] * w + rwx[j];
+    const bool ok = e < N && f >= 0 && f < n;
+    ru[j] = ok ? in.u[f] : 0.f;
+    rpx[j] = ok ? in.px[f] : 0.f;
+    rpy[j] = ok ? in.py[f] : 0.f;
     if (e < N) {
       sUB[e] = ok ? in.ub[f] : 0.f;
       sVX[e] = ok ? in.vbx[f] : 0.f;
