@@ -4,21 +4,26 @@
 // vfs_grad_forward runs a plan's solve (Python/vfs.py:460-533) on float
 // images and a translation t, then the depth map of triangulate_flow
 // (Python/vfs.py:535-559), recording a tape: per warp the flow, u and u_ at
-// its start, and the solver state every `ckpt` iterations.
-// vfs_grad_backward takes the cotangent of the depth map and returns the
-// cotangents of both images, of t and of theta = (Lambda, alpha0, alpha1,
-// beta, gamma).
+// its start, and the solver state at the end of every `ckpt`-iteration
+// interval (with ckpt 1, every state, written by the recording form of the
+// blocked TGV kernel).  vfs_grad_backward takes the cotangent of the depth
+// map and returns the cotangents of both images, of t and of theta =
+// (Lambda, alpha0, alpha1, beta, gamma).
 //
 // Backward schedule, per level from fine to coarse and per warp from last to
-// first: recompute the warp's constants and tvec from the tape, then for each
-// checkpoint interval from last to first recompute its states one iteration
-// per launch and reverse them with three gather kernels per iteration
-// (k_rev1: primal and threshold adjoints, pixel-local; k_rev2: dual adjoint,
-// reads k_rev1's values at the E and S flat neighbours; k_rev3: the
-// transposed gradients of u_ and v_, reads k_rev2's values at the four flat
-// neighbours).  The outer stages have one kernel each; transposed texture
-// fetches scatter with float atomics.  Scalar cotangents are block-reduced and
-// added to a device double[8] (t0 t1 t2 Lambda alpha0 alpha1 beta gamma).
+// first: recompute the warp's constants and tvec from the tape, reverse the
+// median/clamp, then for each checkpoint interval from last to first
+// recompute the states between its ends (recording kernel) and reverse its
+// iterations.  An iteration reverses in three phases: primal and threshold
+// adjoints (pixel-local), the dual adjoint (gathers phase-1 values at the E
+// and S flat neighbours), the transposed gradients of u_ and v_ (gathers
+// phase-2 values at the four flat neighbours).  The default form,
+// k_rev_block, runs them for 2-4 iterations per launch on shared-memory
+// tiles; k_rev_tile (one iteration per launch) and k_rev1/2/3 (one kernel
+// per phase) are the simpler forms, kept selectable and tested against it.
+// The outer stages have one kernel each; transposed texture fetches scatter
+// with float atomics.  Scalar cotangents are block-reduced and added to a
+// device double[8] (t0 t1 t2 Lambda alpha0 alpha1 beta gamma).
 //
 // Rules at the non-smooth points: a texture fetch differentiates exact
 // bilinear interpolation at the fetch coordinate (the hardware's 8-bit
