@@ -1094,7 +1094,29 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       scode[e] = ok ? r.c.code[f] : 0;
     }
   }
+  // with the tile and a one-pixel ring around it all masked, every phase-2
+  // value the tile gathers is zero and so is its cotangent: write that
+  int live = 0;
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int e = threadIdx.x + j * NT;
+    if (e < N && rx[j] >= -1 && rx[j] <= TX && ry[j] >= -1 && ry[j] <= TY && (scode[e] & kSelf)) live = 1;
+  }
+  live = __syncthreads_or(live);
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  if (!live) {
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      if (rx[j] < 0 || rx[j] >= TX || ry[j] < 0 || ry[j] >= TY) continue;
+      const int X = x0 + rx[j], Y = y0 + ry[j];
+      if (X >= w || Y >= h) continue;
+      const long f = (long)Y * w + X;
+      r.g_out.u[f] = r.g_out.ub[f] = r.g_out.vbx[f] = r.g_out.vby[f] = r.g_out.px[f] = r.g_out.py[f] = 0.f;
+      r.g_out.qx[f] = r.g_out.qy[f] = r.g_out.qz[f] = r.g_out.qw[f] = 0.f;
+    }
+    cp_async_wait<0>();
+    return;
+  }
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int e = threadIdx.x + j * NT;

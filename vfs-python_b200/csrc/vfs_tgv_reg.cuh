@@ -75,7 +75,33 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     riz[j] = ok ? cst.iz[f] : 0.f;
     rcode[j] = ok ? cst.code[f] : 0;
   }
+  // a tile whose pixels are all masked ends with zero state (masked pixels
+  // are written 0 every iteration): write that and skip the iterations
+  int live = 0;
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int tx = rwx[j] - 2 * K, ty = rwy[j] - 2 * K;
+    if (tx >= 0 && tx < TX && ty >= 0 && ty < TY && x0 + tx < w && y0 + ty < h && (rcode[j] & kSelf)) live = 1;
+  }
+  live = __syncthreads_or(live);
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  if (!live) {
+    const int k0 = niter < K ? niter : K;
+    for (int s = 0; s < (TRACE ? k0 : 1); ++s) {
+      const TgvState o = TRACE ? trace[s] : out;
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int tx = rwx[j] - 2 * K, ty = rwy[j] - 2 * K;
+        if (tx < 0 || tx >= TX || ty < 0 || ty >= TY) continue;
+        const int X = x0 + tx, Y = y0 + ty;
+        if (X >= w || Y >= h) continue;
+        const long f = (long)Y * w + X;
+        o.u[f] = o.ub[f] = o.vbx[f] = o.vby[f] = o.px[f] = o.py[f] = 0.f;
+        o.qx[f] = o.qy[f] = o.qz[f] = o.qw[f] = 0.f;
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int e = threadIdx.x + j * NT;
