@@ -206,3 +206,27 @@ def test_oracle_end_to_end_default_params(gold):
     m = gold["mask"] > 0
     d = np.abs(warp - gold["e2e_default_warp"])[m]
     assert np.median(d) < 1e-3 and np.percentile(d, 99) < 0.05, (np.median(d), np.percentile(d, 99))
+
+
+def test_grad_workspace_size_and_validation(lib):
+    """Reverse-mode plan sizing (no GPU needed): recording every state costs
+    about ckpt_every times the checkpointed tape; bad arguments are rejected
+    before any CUDA call."""
+    n1, n10 = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    prm = _prm(lib)
+    lib.call("vfs_grad_workspace_size", ctypes.byref(prm), 1, ctypes.byref(n1))
+    lib.call("vfs_grad_workspace_size", ctypes.byref(prm), 10, ctypes.byref(n10))
+    plan = ctypes.c_size_t(0)
+    lib.call("vfs_plan_workspace_size", ctypes.byref(prm), ctypes.byref(plan))
+    assert n1.value > 4 * n10.value > 4 * plan.value
+    with pytest.raises(ValueError):
+        lib.call("vfs_grad_workspace_size", ctypes.byref(prm), 0, ctypes.byref(n1))
+    with pytest.raises(ValueError):
+        lib.call("vfs_grad_workspace_size", ctypes.byref(_prm(lib, nLevel=0)), 10, ctypes.byref(n1))
+    gp = ctypes.c_void_p(0)
+    rc = lib.lib().vfs_grad_create(ctypes.byref(prm), 10, 100.0, 32.0, 32.0, 1.0, None, 0, ctypes.byref(gp))
+    assert rc == lib.VFS_ERR_WORKSPACE
+    rc = lib.lib().vfs_grad_create(ctypes.byref(prm), 10, 0.0, 32.0, 32.0, 1.0, None, 0, ctypes.byref(gp))
+    assert rc == lib.VFS_ERR_ARG  # focal length must be positive
+    assert lib.lib().vfs_grad_set_options(None, 11, 0) == lib.VFS_ERR_ARG
+    assert lib.lib().vfs_grad_backward(None, None, None, None, None, None) == lib.VFS_ERR_ARG
