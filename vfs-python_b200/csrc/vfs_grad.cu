@@ -942,12 +942,13 @@ bool rev_shape_ok(int shape) {
 // ---------------------------------------------------------------- blocked reverse
 // k (<= K) reverse iterations per launch: from the cotangent of S_{i0+k} to
 // that of S_{i0}, reading the recorded states S_{i0} .. S_{i0+k}.  The same
-// three phases per step as k_rev_tile; the cotangent state stays in the
-// registers of the thread that owns its window pixel and the constant
-// cotangents accumulate in shared memory, so cotangents and constants cross
-// HBM once per launch instead of once per iteration.  The recorded states
-// stream into three shared-memory buffers with cp.async: while step m runs
-// on S_{i0+k-m} and S_{i0+k-m+1}, the state of step m+1 is already loading.
+// three phases per step as k_rev_tile.  Each thread owns one window pixel:
+// its cotangent state and, on the tile, its constant cotangents stay in the
+// thread's registers, so cotangents and constants cross HBM once per launch
+// instead of once per iteration.  The recorded states stream into three
+// shared-memory buffers with cp.async: while step m runs on S_{i0+k-m} and
+// S_{i0+k-m+1}, the state of step m+1 is already loading.  Two barriers per
+// step: phase 3 and the next step's phase 1 share one interval.
 //
 // Geometry.  Step m (1..k) produces a valid cotangent on O_m = [-(k-m),
 // T + 2(k-m)) in tile coordinates (phase 3 there; phase 2 on O_m grown by 1,
@@ -986,7 +987,7 @@ struct RbGeom {
   static constexpr int LHX = (K + 1 + 3) / 4 * 4;
   static constexpr int WX = (TX + LHX + 2 * K + 3) / 4 * 4, WY = TY + 3 * K + 1, N = WX * WY;
   static constexpr size_t smem_bytes() {
-    return (size_t)kRbPlanes * N * 4 + (size_t)8 * TX * TY * 4 + ((N + 15) / 16) * 16;
+    return (size_t)kRbPlanes * N * 4 + ((N + 15) / 16) * 16;
   }
 };
 
@@ -1006,11 +1007,10 @@ template <int K, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   using G = RbGeom<K, TX, TY>;
   static_assert(G::N <= NT, "one window pixel per thread");
-  constexpr int WX = G::WX, N = G::N, LH = G::LH, LHX = G::LHX, J = (N + NT - 1) / NT, TT = TX * TY;
+  constexpr int WX = G::WX, N = G::N, LH = G::LH, LHX = G::LHX, J = (N + NT - 1) / NT;
   extern __shared__ float4 smem_raw[];
   float* const sm = reinterpret_cast<float*>(smem_raw);
-  float* const sgc = sm + (size_t)kRbPlanes * N;
-  uint8_t* const scode = reinterpret_cast<uint8_t*>(sgc + 8 * TT);
+  uint8_t* const scode = reinterpret_cast<uint8_t*>(sm + (size_t)kRbPlanes * N);
   auto P = [&](int plane) { return sm + (size_t)plane * N; };
   const int w = r.w, h = r.h;
   const long n = (long)h * w;
@@ -1021,6 +1021,10 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   const float eps = 1E-7f;
   const float al0 = r.k.alpha0, al1 = r.k.alpha1, lam = r.k.lambda;
   float acc[3] = {0.f, 0.f, 0.f};  // Lambda, alpha0, alpha1
+  // constant cotangents of the thread's tile pixel over this launch's steps
+  // (one window pixel per thread: J == 1)
+  static_assert(J == 1, "one window pixel per thread");
+  float gca[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
   float gU[J], gUB[J], gVX[J], gVY[J], gPX[J], gPY[J], gQ0[J], gQ1[J], gQ2[J], gQ3[J];
   int rx[J], ry[J];
@@ -1133,13 +1137,13 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     gQ2[j] = ok ? r.g_in.qz[f] : 0.f;
     gQ3[j] = ok ? r.g_in.qw[f] : 0.f;
   }
-  for (int q = threadIdx.x; q < 8 * TT; q += NT) sgc[q] = 0.f;
   if (k >= 2) cp_async_wait<1>(); else cp_async_wait<0>();
   __syncthreads();
 
   for (int m = 1; m <= k; ++m) {
     const float3 ss = r.sched[r.i0 + k - m];
     const float sigma = ss.x, tau = ss.y, mu = ss.z;
+    const float sQe = __fdividef(sigma, r.k.etaQ), sPe = __fdividef(sigma, r.k.etaP);  // gradient scales only
     const int lo = -(k - m), hiX = TX + 2 * (k - m), hiY = TY + 2 * (k - m);
     const int L0 = bS0 + (m % 3) * kStPlanes, H0 = bS0 + ((m - 1) % 3) * kStPlanes;  // later / earlier state
     // phase 1: primal and threshold reversed on [lo - 1, hi + 2)
@@ -1210,14 +1214,13 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
         lVX[j] = gVx - mu * gvbx;
         lVY[j] = gVy - mu * gvby;
         if (core) {
-          const int ci = ry[j] * TX + rx[j];
           const float inx = fmaf(al1, tpx, al0 * (gQx + gQz));
           const float iny = fmaf(al1, tpy, al0 * (gQw + gQy));
-          sgc[3 * TT + ci] -= te * rex * gte;
-          sgc[4 * TT + ci] -= t1 * rey * inx * gVx;
-          sgc[5 * TT + ci] -= t2 * rez * iny * gVy;
-          sgc[6 * TT + ci] += giu;
-          sgc[7 * TT + ci] += giz;
+          gca[3] -= te * rex * gte;
+          gca[4] -= t1 * rey * inx * gVx;
+          gca[5] -= t2 * rez * iny * gVy;
+          gca[6] += giu;
+          gca[7] += giz;
           acc[0] += gl;
           acc[1] += t1 * (gQx + gQz) * gVx + t2 * (gQw + gQy) * gVy;
           acc[2] += t1 * tpx * gVx + t2 * tpy * gVy;
@@ -1316,22 +1319,26 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
         nQ2[j] = gq2;
         nQ3[j] = gq3;
         if (core) {
-          const int ci = ry[j] * TX + rx[j];
-          sgc[0 * TT + ci] += ga + gUx * gtux;
-          sgc[1 * TT + ci] += gb + gUy * gtuy;
-          sgc[2 * TT + ci] += gcc + gUy * gtux + gUx * gtuy;
-          acc[1] += sigma / r.k.etaQ * (gVxx * gq0 + gVyy * gq1 + gVz * gq2 + gVw * gq3);
-          acc[2] += sigma / r.k.etaP * (tux * gP0 + tuy * gP1);
+          gca[0] += ga + gUx * gtux;
+          gca[1] += gb + gUy * gtuy;
+          gca[2] += gcc + gUy * gtux + gUx * gtuy;
+          acc[1] += sQe * (gVxx * gq0 + gVyy * gq1 + gVz * gq2 + gVw * gq3);
+          acc[2] += sPe * (tux * gP0 + tuy * gP1);
         }
       }
 #pragma unroll
       for (int q = 0; q < 6; ++q) P(bC0 + q)[e] = Cv[q];
     }
+    // phase 3 and the next step's phase 1 share one barrier interval: the
+    // state that phase 1 reads first (loaded a step ahead) is waited for here
+    if (m < k) cp_async_wait<0>();
     __syncthreads();
     // the later state's buffer is no longer read: the state of step m + 2
-    // starts loading into it while phase 3 runs
+    // starts loading into it
     if (m + 2 <= k) load_state(k - m - 2, (m + 2) % 3);
-    // phase 3: transposed gradients of u_ and v_ on [lo, hi); commit the step
+    // phase 3: transposed gradients of u_ and v_ on [lo, hi); commit the step.
+    // It reads the phase-2 results only; the next phase 1 writes the phase-1
+    // planes (last read in phase 2) and reads states waited for above.
 #pragma unroll
     for (int j = 0; j < J; ++j) {
       if (rx[j] < lo || rx[j] >= hiX || ry[j] < lo || ry[j] >= hiY) continue;
@@ -1376,13 +1383,6 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       gQ2[j] = nQ2[j];
       gQ3[j] = nQ3[j];
     }
-    // wait for the state of step m + 1
-    if (m + 2 <= k) {
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
   }
 
   // cotangent of S_{i0} on the tile; constant cotangents added to HBM once
@@ -1402,17 +1402,9 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     r.g_out.qy[f] = gQ1[j];
     r.g_out.qz[f] = gQ2[j];
     r.g_out.qw[f] = gQ3[j];
-  }
-  for (int ci = threadIdx.x; ci < TT; ci += NT) {
-    const int cy = ci / TX, cx = ci - cy * TX;
-    const int X = x0 + cx, Y = y0 + cy;
-    if (X >= w || Y >= h) continue;
-    const long f = (long)Y * w + X;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const float v = sgc[q * TT + ci];
-      if (v != 0.f) r.gc[q][f] += v;
-    }
+    for (int q = 0; q < 8; ++q)
+      if (gca[q] != 0.f) r.gc[q][f] += gca[q];
   }
   block_sum_to<3>(acc, r.scal + G_LAMBDA);
 }
@@ -1739,7 +1731,6 @@ struct VfsGradPlan {
     float* ub_in;
     float2* warp_in;
     std::vector<TgvState> ck;  // state after iterations ckpt, 2 ckpt, ..., nSolverIters
-    TgvState* d_ck;            // device copy of ck (recording targets)
     TgvState* d_seg;           // per checkpoint interval, its states (segment_lists)
   };
   std::vector<std::vector<Warp>> tape;
@@ -1755,7 +1746,6 @@ struct VfsGradPlan {
   std::vector<float*> gref, gother;
   std::vector<float2*> gtvf;
   double* scal = nullptr;
-  TgvState* d_slot = nullptr;  // device copy of `slot` (recording targets)
   int fused_reverse = 11;  // reverse-step kernel form (vfs_grad_set_options)
   // instrumentation: an event pair around each interval's reverse launches
   bool timing = false;
@@ -1825,7 +1815,6 @@ size_t grad_layout(VfsGradPlan* gp, const VfsParams* p, char* base) {
       wt.warp_in = cv.take<float2>(n * 8);
       wt.ck.resize(std::max(0, nck));
       for (auto& s : wt.ck) take_state(cv, &s, n);
-      wt.d_ck = cv.take<TgvState>(std::max(1, nck) * sizeof(TgvState));
       wt.d_seg = cv.take<TgvState>(seg_entries(gp, p) * sizeof(TgvState));
     }
   }
@@ -1855,7 +1844,6 @@ size_t grad_layout(VfsGradPlan* gp, const VfsParams* p, char* base) {
     gp->gtvf[l] = cv.take<float2>(n * 8);
   }
   gp->scal = cv.take<double>(G_NSCAL * sizeof(double));
-  gp->d_slot = cv.take<TgvState>((gp->ckpt + 1) * sizeof(TgvState));
   return cv.off + kGAlign;
 }
 
@@ -1871,6 +1859,25 @@ std::vector<TgvState> interval_states(const VfsGradPlan* gp, const VfsGradPlan::
   for (int q = 1; q < nj; ++q) S[q] = gp->slot[q];
   if (nj > 0) S[nj] = wt.ck[j];
   return S;
+}
+
+// The distance in floats between consecutive state sets v[i0 .. i0 + m),
+// when every plane moves by the same amount (the recording kernel's trace
+// layout); false if they do not.
+bool record_stride(const std::vector<TgvState>& v, int i0, int m, long* stride) {
+  *stride = 0;
+  if (i0 < 0 || m < 1 || i0 + m > (int)v.size()) return false;
+  if (m == 1) return true;
+  const long d = v[i0 + 1].u - v[i0].u;
+  for (int r = i0; r + 1 < i0 + m; ++r) {
+    const TgvState &a = v[r], &b = v[r + 1];
+    const float* pa[10] = {a.u, a.ub, a.vbx, a.vby, a.px, a.py, a.qx, a.qy, a.qz, a.qw};
+    const float* pb[10] = {b.u, b.ub, b.vbx, b.vby, b.px, b.py, b.qx, b.qy, b.qz, b.qw};
+    for (int q = 0; q < 10; ++q)
+      if (pb[q] - pa[q] != d) return false;
+  }
+  *stride = d;
+  return true;
 }
 
 // All interval state lists of a warp, in the layout of Warp::d_seg.
@@ -1963,7 +1970,9 @@ int grad_forward(VfsGradPlan* gp, const float* img_ref, const float* img_other, 
         const int K = tgv_max_iters_per_launch(tv);
         while (it < nI) {
           const int m = std::min(K, nI - it);
-          VFS_TRY_CUDA(launch_tgv_trace(tv, cur, wt.d_ck + it, c.cst, pl->sched, it, m, pl->kc, h, w, s), "tgv");
+          long rs;
+          if (!record_stride(wt.ck, it, m, &rs)) return fail(VFS_ERR_WORKSPACE, "tape records not evenly spaced");
+          VFS_TRY_CUDA(launch_tgv_trace(tv, cur, wt.ck[it], rs, c.cst, pl->sched, it, m, pl->kc, h, w, s), "tgv");
           cur = wt.ck[it + m - 1];
           it += m;
         }
@@ -2100,9 +2109,11 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
           if (tv) {
             for (int q = 0; q < nj - 1;) {
               const int m = std::min(tgv_max_iters_per_launch(tv), nj - 1 - q);
-              VFS_TRY_CUDA(
-                  launch_tgv_trace(tv, S[q], gp->d_slot + q + 1, cst, pl->sched, it0 + q, m, pl->kc, h, w, s),
-                  "tgv recompute");
+              long rs;
+              if (!record_stride(gp->slot, q + 1, m, &rs))
+                return fail(VFS_ERR_WORKSPACE, "recomputation slots not evenly spaced");
+              VFS_TRY_CUDA(launch_tgv_trace(tv, S[q], gp->slot[q + 1], rs, cst, pl->sched, it0 + q, m, pl->kc, h, w, s),
+                           "tgv recompute");
               q += m;
             }
           } else {
@@ -2268,11 +2279,9 @@ int vfs_grad_create(const VfsParams* prm, int ckpt_every, float f, float u0, flo
   step_schedule(prm->nSolverIters, prm->timeStepLambda, gp->sched.data());
   char* gbase = reinterpret_cast<char*>(gru(reinterpret_cast<uintptr_t>(base + gru(pb, kGAlign)), kGAlign));
   grad_layout(gp, prm, gbase);
-  cudaError_t e = cudaMemcpy(gp->d_slot, gp->slot.data(), gp->slot.size() * sizeof(TgvState), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaSuccess;
   for (auto& lvl : gp->tape)
     for (auto& wt : lvl) {
-      if (e == cudaSuccess && !wt.ck.empty())
-        e = cudaMemcpy(wt.d_ck, wt.ck.data(), wt.ck.size() * sizeof(TgvState), cudaMemcpyHostToDevice);
       if (e == cudaSuccess) {
         const std::vector<TgvState> seg = segment_lists(gp, wt, prm->nSolverIters);
         e = cudaMemcpy(wt.d_seg, seg.data(), seg.size() * sizeof(TgvState), cudaMemcpyHostToDevice);

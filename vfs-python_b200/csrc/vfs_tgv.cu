@@ -343,17 +343,17 @@ bool tgv_has_trace(int variant) {
   }
 }
 
-cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState* trace, const TgvConsts& c,
-                             const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
-                             cudaStream_t s) {
+cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState& trace0, long rec_stride,
+                             const TgvConsts& c, const float3* sched, int it0, int niter, const SolverConsts& kc,
+                             int h, int w, cudaStream_t s) {
   if (h <= 0 || w <= 0 || niter <= 0) return cudaSuccess;
   switch (variant) {
 #define VFS_LAUNCH_T(id, K, TX, TY, NT)                                                                    \
   case id: {                                                                                               \
     if (niter > K) return cudaErrorInvalidValue;                                                           \
     PdlLaunch L(dim3((w + TX - 1) / TX, (h + TY - 1) / TY), NT, RegGeom<K, TX, TY>::smem_bytes(), s);     \
-    return cudaLaunchKernelEx(&L.cfg, k_tgv_reg_trace<K, TX, TY, NT>, in, trace, c, sched, it0, niter, kc, h, \
-                              w);                                                                          \
+    return cudaLaunchKernelEx(&L.cfg, k_tgv_reg_trace<K, TX, TY, NT>, in, trace0, rec_stride, c, sched, it0, \
+                              niter, kc, h, w);                                                            \
   }
     VFS_TGV_TRACE_VARIANTS(VFS_LAUNCH_T)
 #undef VFS_LAUNCH_T

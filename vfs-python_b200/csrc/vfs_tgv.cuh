@@ -57,11 +57,12 @@ cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& ou
 
 // Recording form of a register-owned variant (tgv_has_trace): runs `niter`
 // (<= K) iterations from `in` and writes the state after iteration s to
-// trace[s - 1] (an array of state sets in device memory).
+// record s - 1 of the trace: the state set whose planes are those of trace0
+// moved by (s - 1) * rec_stride floats.
 bool tgv_has_trace(int variant);
-cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState* trace, const TgvConsts& c,
-                             const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
-                             cudaStream_t s);
+cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState& trace0, long rec_stride,
+                             const TgvConsts& c, const float3* sched, int it0, int niter, const SolverConsts& kc,
+                             int h, int w, cudaStream_t s);
 
 // Cluster-resident solve of a whole level (vfs_tgv_cluster.cu): all `niter`
 // iterations, then median filter and clamped flow update, in one launch of a

@@ -25,13 +25,14 @@ struct RegGeom {
 };
 
 // One CTA's tile whose origin is (x0, y0).
-// With TRACE, the state after iteration s (of this launch) is written to
-// trace[s - 1] instead of the final state to `out`.
+// With TRACE, the state after iteration s (of this launch) is written to the
+// record s - 1 of the trace, whose planes are those of `out` moved by
+// (s - 1) * rec_stride floats, instead of the final state to `out`.
 template <int K, int TX, int TY, int NT, bool TRACE = false>
 __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState& out, const TgvConsts& cst,
                                              const float3* __restrict__ sched, int it0, int niter,
                                              const SolverConsts& kc, int h, int w, int x0, int y0,
-                                             const TgvState* __restrict__ trace = nullptr) {
+                                             long rec_stride = 0) {
   using G = RegGeom<K, TX, TY>;
   constexpr int WX = G::WX, N = G::N, J = (N + NT - 1) / NT;
   extern __shared__ float4 smem_raw[];
@@ -88,16 +89,16 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   if (!live) {
     const int k0 = niter < K ? niter : K;
     for (int s = 0; s < (TRACE ? k0 : 1); ++s) {
-      const TgvState o = TRACE ? trace[s] : out;
+      const long ro = (long)s * rec_stride;
 #pragma unroll
       for (int j = 0; j < J; ++j) {
         const int tx = rwx[j] - 2 * K, ty = rwy[j] - 2 * K;
         if (tx < 0 || tx >= TX || ty < 0 || ty >= TY) continue;
         const int X = x0 + tx, Y = y0 + ty;
         if (X >= w || Y >= h) continue;
-        const long f = (long)Y * w + X;
-        o.u[f] = o.ub[f] = o.vbx[f] = o.vby[f] = o.px[f] = o.py[f] = 0.f;
-        o.qx[f] = o.qy[f] = o.qz[f] = o.qw[f] = 0.f;
+        const long f = (long)Y * w + X + ro;
+        out.u[f] = out.ub[f] = out.vbx[f] = out.vby[f] = out.px[f] = out.py[f] = 0.f;
+        out.qx[f] = out.qy[f] = out.qz[f] = out.qw[f] = 0.f;
       }
     }
     return;
@@ -188,7 +189,7 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
       }
     }
     if constexpr (TRACE) {  // each thread writes the tile pixels it owns
-      const TgvState o = trace[s - 1];
+      const long ro = (long)(s - 1) * rec_stride;
 #pragma unroll
       for (int j = 0; j < J; ++j) {
         const int tx = rwx[j] - 2 * K, ty = rwy[j] - 2 * K;
@@ -196,17 +197,17 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
         const int X = x0 + tx, Y = y0 + ty;
         if (X >= w || Y >= h) continue;
         const int i = threadIdx.x + j * NT;
-        const long f = (long)Y * w + X;
-        o.u[f] = ru[j];
-        o.ub[f] = sUB[i];
-        o.vbx[f] = sVX[i];
-        o.vby[f] = sVY[i];
-        o.px[f] = rpx[j];
-        o.py[f] = rpy[j];
-        o.qx[f] = sQX[i];
-        o.qy[f] = sQY[i];
-        o.qz[f] = sQZ[i];
-        o.qw[f] = sQW[i];
+        const long f = (long)Y * w + X + ro;
+        out.u[f] = ru[j];
+        out.ub[f] = sUB[i];
+        out.vbx[f] = sVX[i];
+        out.vby[f] = sVY[i];
+        out.px[f] = rpx[j];
+        out.py[f] = rpy[j];
+        out.qx[f] = sQX[i];
+        out.qy[f] = sQY[i];
+        out.qz[f] = sQZ[i];
+        out.qw[f] = sQW[i];
       }
     }
     __syncthreads();
@@ -243,13 +244,14 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
   tgv_reg_tile<K, TX, TY, NT>(in, out, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY);
 }
 
-// Recording: every iteration's state to trace[0..niter).
+// Recording: every iteration's state to the records 0..niter of the trace
+// (record r: the planes of trace0 moved by r * rec_stride floats).
 template <int K, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
-    k_tgv_reg_trace(TgvState in, const TgvState* __restrict__ trace, TgvConsts cst, const float3* __restrict__ sched,
+    k_tgv_reg_trace(TgvState in, TgvState trace0, long rec_stride, TgvConsts cst, const float3* __restrict__ sched,
                     int it0, int niter, SolverConsts kc, int h, int w) {
-  tgv_reg_tile<K, TX, TY, NT, true>(in, in, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY,
-                                    trace);
+  tgv_reg_tile<K, TX, TY, NT, true>(in, trace0, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY,
+                                    rec_stride);
 }
 
 // Batched: one launch over the tiles of many images (the pairs of a batch at
