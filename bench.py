@@ -102,6 +102,13 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: wait for its first row (taken
+            # before the timed region, so dropped) so that the 200 ms samples
+            # cover the whole timed region
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 10 and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.rows.clear()
         except Exception:
             self.proc = None
         return self
@@ -713,7 +720,9 @@ def run_grad(args, n, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 40 for single, 10 for batched and grad, 3 for learn; "
+                         "10 for --impl reference)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--iters-per-launch", type=int, default=134)
@@ -738,6 +747,9 @@ def main():
                          "kernel --iters-per-launch everywhere (1000: cluster kernel), no graph; two solves")
     ap.add_argument("--profile-size", type=int, default=SIZE)
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 10 if args.impl == "reference" else {"single": 40, "batched": 10, "grad": 10,
+                                                            "learn": 3}[args.workload]
     args.warmup = max(args.warmup, 1)
     if args.profile_case and args.profile_grad:
         torch.cuda.set_device(0)

@@ -69,7 +69,22 @@ inline SolverConsts make_consts(const VfsParams* p) {
   k.a11 = (float)(p->alpha1 * p->alpha1);
   k.fscale = (float)p->fScale;
   k.upperLimit = (float)p->limitRange;
+  k.dscale = nullptr;
   return k;
+}
+
+// The dual step's scales for each iteration of a (sigma, tau, mu) schedule:
+// alpha1 * sigma / etaP and alpha0 * sigma / etaQ, the float32 multiply then
+// divide of the dual step (Python/vfs.cu:370-371).  IEEE single-precision
+// multiply and divide round the same on the host as on the device, so these
+// equal the kernels' own evaluation bit for bit.
+inline void dual_scales(const SolverConsts& k, const float* sched3, int n, float* out2) {
+  for (int i = 0; i < n; ++i) {
+    const float sigma = sched3[3 * i];
+    const float a1s = k.alpha1 * sigma, a0s = k.alpha0 * sigma;
+    out2[2 * i] = a1s / k.etaP;
+    out2[2 * i + 1] = a0s / k.etaQ;
+  }
 }
 
 // (sigma, tau, mu) for each solver iteration, as the reference's host loop

@@ -1144,6 +1144,7 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     const float3 ss = r.sched[r.i0 + k - m];
     const float sigma = ss.x, tau = ss.y, mu = ss.z;
     const float sQe = __fdividef(sigma, r.k.etaQ), sPe = __fdividef(sigma, r.k.etaP);  // gradient scales only
+    const float2 dsc = r.k.dscale[r.i0 + k - m];  // the forward's dual-step scales
     const int lo = -(k - m), hiX = TX + 2 * (k - m), hiY = TY + 2 * (k - m);
     const int L0 = bS0 + (m % 3) * kStPlanes, H0 = bS0 + ((m - 1) % 3) * kStPlanes;  // later / earlier state
     // phase 1: primal and threshold reversed on [lo - 1, hi + 2)
@@ -1283,23 +1284,27 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
           gVyy = vcy - lvy[e - WX];
           gVz = vcx - lvx[e - WX];
         }
-        const float scaleP = al1 * sigma / r.k.etaP;
-        const float scaleQ = al0 * sigma / r.k.etaQ;
+        const float scaleP = dsc.x, scaleQ = dsc.y;
         const float tux = fmaf(a, gUx, cc * gUy), tuy = fmaf(cc, gUx, b * gUy);
         const float upx = fmaf(scaleP, tux, P(L0 + sPX)[e]), upy = fmaf(scaleP, tuy, P(L0 + sPY)[e]);
-        const float nP = hypotf(upx, upy);
+        // A projection was active where the recorded result differs from its
+        // recomputed argument: the forward returns an inactive argument bit
+        // for bit, an active one divided by a norm > 1.  NaN arguments count
+        // as inactive (the forward's norm > 1 is false for them).  The
+        // reciprocal norm only scales cotangents: rsqrt of the squared norm.
         float gP0 = gpx, gP1 = gpy;
-        if (nP > 1.f) {
-          const float dt = pnx * gpx + pny * gpy, rn = __fdividef(1.f, nP);
+        if ((pnx != upx || pny != upy) && upx == upx && upy == upy) {
+          const float dt = pnx * gpx + pny * gpy, rn = rsqrtf(fmaf(upx, upx, upy * upy));
           gP0 = (gpx - pnx * dt) * rn;
           gP1 = (gpy - pny * dt) * rn;
         }
         const float uq0 = fmaf(scaleQ, gVxx, P(L0 + sQX)[e]), uq1 = fmaf(scaleQ, gVyy, P(L0 + sQY)[e]);
         const float uq2 = fmaf(scaleQ, gVz, P(L0 + sQZ)[e]), uq3 = fmaf(scaleQ, gVw, P(L0 + sQW)[e]);
-        const float nQ = norm4df(uq0, uq1, uq2, uq3);
-        if (nQ > 1.f) {
-          const float q0 = P(H0 + sQX)[e], q1 = P(H0 + sQY)[e], q2 = P(H0 + sQZ)[e], q3 = P(H0 + sQW)[e];
-          const float dt = q0 * gq0 + q1 * gq1 + q2 * gq2 + q3 * gq3, rn = __fdividef(1.f, nQ);
+        const float q0 = P(H0 + sQX)[e], q1 = P(H0 + sQY)[e], q2 = P(H0 + sQZ)[e], q3 = P(H0 + sQW)[e];
+        if ((q0 != uq0 || q1 != uq1 || q2 != uq2 || q3 != uq3) && uq0 == uq0 && uq1 == uq1 && uq2 == uq2 &&
+            uq3 == uq3) {
+          const float dt = q0 * gq0 + q1 * gq1 + q2 * gq2 + q3 * gq3,
+                      rn = rsqrtf(fmaf(uq0, uq0, fmaf(uq1, uq1, fmaf(uq2, uq2, uq3 * uq3))));
           gq0 = (gq0 - q0 * dt) * rn;
           gq1 = (gq1 - q1 * dt) * rn;
           gq2 = (gq2 - q2 * dt) * rn;
@@ -1424,6 +1429,7 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 // when that launch wrote none of the recorded states this one reads before
 // its griddepcontrol.wait, i.e. not right after a recomputation).
 cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s, bool pdl) {
+  if (!r.k.dscale) return cudaErrorInvalidValue;  // dual-step scales not formed
   switch (shape) {
 #define VFS_REVB_L(ID, K, TX, TY, NT)                                              \
   case ID: {                                                                       \
@@ -2368,6 +2374,8 @@ int vfs_grad_forward(VfsGradPlan* gp, const float* img_ref, const float* img_oth
   pl->prm = p;
   pl->kc = make_consts(&p);
   pl->drop_graph();
+  VFS_TRY_CUDA(plan_set_dual_scales(pl, (cudaStream_t)stream ? (cudaStream_t)stream : cudaStreamLegacy),
+               "dual-step scales");
   for (int k = 0; k < 3; ++k) gp->t[k] = t[k];
   gp->recorded = false;
   VFS_TRY(grad_forward(gp, img_ref, img_other, depth_out, (cudaStream_t)stream));

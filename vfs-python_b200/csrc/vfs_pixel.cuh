@@ -27,6 +27,10 @@ struct SolverConsts {
   float beta, gamma, minGrad, minTensor;
   float a004, a11;  // 4*alpha0*alpha0 and alpha1*alpha1 (double, then float)
   float fscale, upperLimit;
+  // per solver iteration, (alpha1 sigma / etaP, alpha0 sigma / etaQ): the
+  // dual step's scales, formed once on the host (device memory; read by the
+  // register-owned TGV kernels and the blocked reverse)
+  const float2* dscale;
 };
 
 // ---------------------------------------------------------------- K7 tensor

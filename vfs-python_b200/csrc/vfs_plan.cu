@@ -136,6 +136,7 @@ size_t layout(VfsPlan* pl, char* base) {
     pl->warp[b] = {cv.take<float2>(pitch_of(w0, 8) * h0), pitch_of(w0, 8)};
   }
   pl->sched = cv.take<float3>(sizeof(float3) * std::max(1, pl->prm.nSolverIters));
+  pl->dscale = cv.take<float2>(sizeof(float2) * std::max(1, pl->prm.nSolverIters));
   pl->stage_ref = cv.take<uint8_t>(n0);
   pl->stage_other = cv.take<uint8_t>(n0);
   pl->cst = {pl->cplanes[0], pl->cplanes[1], pl->cplanes[2], pl->cplanes[3], pl->cplanes[4],
@@ -159,6 +160,18 @@ void init_levels(VfsPlan* pl) {
 }  // namespace
 
 namespace vfs {
+
+cudaError_t plan_set_dual_scales(VfsPlan* pl, cudaStream_t s) {
+  const int n = std::max(1, pl->prm.nSolverIters);
+  std::vector<float> sched(3 * n, 0.f);
+  step_schedule(pl->prm.nSolverIters, pl->prm.timeStepLambda, sched.data());
+  pl->dscale_host.assign(2 * n, 0.f);
+  dual_scales(pl->kc, sched.data(), n, pl->dscale_host.data());
+  pl->kc.dscale = pl->dscale;
+  const size_t bytes = pl->dscale_host.size() * sizeof(float);
+  return s ? cudaMemcpyAsync(pl->dscale, pl->dscale_host.data(), bytes, cudaMemcpyHostToDevice, s)
+           : cudaMemcpy(pl->dscale, pl->dscale_host.data(), bytes, cudaMemcpyHostToDevice);
+}
 
 // create_image_pyramid, Python/vfs.py:121-157, from the staged images.
 int plan_pyramids(VfsPlan* pl, cudaStream_t s, long long* nk) {
@@ -381,6 +394,7 @@ int vfs_plan_create(const VfsParams* prm, void* workspace, size_t workspace_byte
   std::vector<float> sched(3 * std::max(1, prm->nSolverIters), 0.f);
   step_schedule(prm->nSolverIters, prm->timeStepLambda, sched.data());
   cudaError_t e = cudaMemcpy(pl->sched, sched.data(), sched.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = plan_set_dual_scales(pl, nullptr);
   if (e != cudaSuccess) {
     delete pl;
     return cuda_status(e, "schedule upload");

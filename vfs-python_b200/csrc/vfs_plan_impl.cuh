@@ -32,6 +32,8 @@ struct VfsPlan {
   vfs::Plane<float> ubefore[2];
   vfs::Plane<float2> warp[2];
   float3* sched = nullptr;
+  float2* dscale = nullptr;          // dual-step scales for kc (dual_scales)
+  std::vector<float> dscale_host;    // their source for the last upload
   int variant = 134;
   int level_variant[32] = {0};  // 0: the plan's variant; VFS_TGV_CLUSTER: cluster kernel
   bool mask_set = false, fields_set = false, solved = false;
@@ -79,6 +81,10 @@ struct LevelCtx {
 // The steps of solve_stereo (Python/vfs.py:460-533), enqueued on `s`; nk
 // counts kernel launches.
 int plan_pyramids(VfsPlan* pl, cudaStream_t s, long long* nk);
+// Forms the dual-step scales of pl->kc (dual_scales), uploads them to
+// pl->dscale (synchronous copy when s is null, else ordered on s) and points
+// pl->kc.dscale at them.  Called whenever pl->kc is (re)built.
+cudaError_t plan_set_dual_scales(VfsPlan* pl, cudaStream_t s);
 int plan_level_begin(VfsPlan* pl, int l, LevelCtx* c, cudaStream_t s, long long* nk);
 int plan_warp_pre(VfsPlan* pl, LevelCtx* c, cudaStream_t s, long long* nk);
 int plan_warp_tgv(VfsPlan* pl, LevelCtx* c, cudaStream_t s, long long* nk, unsigned ev_flags);

@@ -347,6 +347,7 @@ cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState& tr
                              const TgvConsts& c, const float3* sched, int it0, int niter, const SolverConsts& kc,
                              int h, int w, cudaStream_t s) {
   if (h <= 0 || w <= 0 || niter <= 0) return cudaSuccess;
+  if (!kc.dscale) return cudaErrorInvalidValue;  // dual-step scales not formed
   switch (variant) {
 #define VFS_LAUNCH_T(id, K, TX, TY, NT)                                                                    \
   case id: {                                                                                               \
@@ -397,6 +398,7 @@ bool tgv_tile_shape(int variant, int* tx, int* ty) {
 cudaError_t launch_tgv_batch(int variant, const TgvBatchItem* items, int n_items, int total_tiles, int parity,
                              const float3* sched, int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
   if (n_items <= 0 || total_tiles <= 0 || niter <= 0) return cudaSuccess;
+  if (!kc.dscale) return cudaErrorInvalidValue;  // dual-step scales not formed
   switch (variant) {
 #define VFS_BATCH_V(id, impl, K, TX, TY, NT) \
   case id: return batch_##impl<K, TX, TY, NT>(items, n_items, total_tiles, parity, sched, it0, niter, kc, s);
@@ -410,6 +412,7 @@ cudaError_t launch_tgv_block(int variant, const TgvState& in, const TgvState& ou
                              const float3* sched, int it0, int niter, const SolverConsts& kc, int h, int w,
                              cudaStream_t s) {
   if (h <= 0 || w <= 0 || niter <= 0) return cudaSuccess;
+  if (!kc.dscale) return cudaErrorInvalidValue;  // dual-step scales not formed
   switch (variant) {
 #define VFS_LAUNCH_V(id, impl, K, TX, TY, NT) \
   case id: return launch_##impl<K, TX, TY, NT>(in, out, c, sched, it0, niter, kc, h, w, s);

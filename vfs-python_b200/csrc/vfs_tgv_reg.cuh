@@ -126,8 +126,8 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   const int k = niter < K ? niter : K;
   for (int s = 1; s <= k; ++s) {
     const float3 ss = sched[it0 + s - 1];  // (sigma, tau, mu)
-    const float scaleP = kc.alpha1 * ss.x / kc.etaP;
-    const float scaleQ = kc.alpha0 * ss.x / kc.etaQ;
+    const float2 dsc = kc.dscale[it0 + s - 1];  // alpha1 sigma / etaP, alpha0 sigma / etaQ
+    const float scaleP = dsc.x, scaleQ = dsc.y;
     {  // dual step on [lo, hiX) x [lo, hiY)
       const int lo = 2 * K - 2 * (k - s) - 1;
       const int hiX = 2 * K + TX + (k - s), hiY = 2 * K + TY + (k - s);
