@@ -987,7 +987,9 @@ struct RbGeom {
   static constexpr int LHX = (K + 1 + 3) / 4 * 4;
   static constexpr int WX = (TX + LHX + 2 * K + 3) / 4 * 4, WY = TY + 3 * K + 1, N = WX * WY;
   static constexpr size_t smem_bytes() {
-    return (size_t)kRbPlanes * N * 4 + ((N + 15) / 16) * 16;
+    // planes, mask codes, then (sigma, tau, mu, scaleP, scaleQ) of each of
+    // the launch's iterations
+    return (size_t)kRbPlanes * N * 4 + ((N + 15) / 16) * 16 + 5 * K * 4;
   }
 };
 
@@ -1011,6 +1013,7 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   extern __shared__ float4 smem_raw[];
   float* const sm = reinterpret_cast<float*>(smem_raw);
   uint8_t* const scode = reinterpret_cast<uint8_t*>(sm + (size_t)kRbPlanes * N);
+  float* const sSch = reinterpret_cast<float*>(scode + ((N + 15) / 16) * 16);
   auto P = [&](int plane) { return sm + (size_t)plane * N; };
   const int w = r.w, h = r.h;
   const long n = (long)h * w;
@@ -1080,6 +1083,11 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   // everything above and the constants below are recorded data; the
   // cotangent it wrote is read only after griddepcontrol.wait
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  if (threadIdx.x < 5 * k) {  // this launch's step sizes and dual-step scales
+    const int t = threadIdx.x / 5, c = threadIdx.x - 5 * t;
+    sSch[threadIdx.x] = c < 3 ? reinterpret_cast<const float*>(r.sched + r.i0 + t)[c]
+                              : reinterpret_cast<const float*>(r.k.dscale + r.i0 + t)[c - 3];
+  }
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int e = threadIdx.x + j * NT;
@@ -1141,10 +1149,10 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   __syncthreads();
 
   for (int m = 1; m <= k; ++m) {
-    const float3 ss = r.sched[r.i0 + k - m];
-    const float sigma = ss.x, tau = ss.y, mu = ss.z;
+    const float* const sc = sSch + 5 * (k - m);
+    const float sigma = sc[0], tau = sc[1], mu = sc[2];
     const float sQe = __fdividef(sigma, r.k.etaQ), sPe = __fdividef(sigma, r.k.etaP);  // gradient scales only
-    const float2 dsc = r.k.dscale[r.i0 + k - m];  // the forward's dual-step scales
+    const float2 dsc = make_float2(sc[3], sc[4]);  // the forward's dual-step scales
     const int lo = -(k - m), hiX = TX + 2 * (k - m), hiY = TY + 2 * (k - m);
     const int L0 = bS0 + (m % 3) * kStPlanes, H0 = bS0 + ((m - 1) % 3) * kStPlanes;  // later / earlier state
     // phase 1: primal and threshold reversed on [lo - 1, hi + 2)

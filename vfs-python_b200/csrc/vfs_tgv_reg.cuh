@@ -21,7 +21,9 @@ struct RegGeom {
   static constexpr int WX = TX + 3 * K;
   static constexpr int WY = TY + 3 * K;
   static constexpr int N = WX * WY;
-  static constexpr size_t smem_bytes() { return (size_t)kRegPlanes * N * sizeof(float); }
+  // the planes, then (sigma, tau, mu, scaleP, scaleQ) of each of the
+  // launch's iterations
+  static constexpr size_t smem_bytes() { return ((size_t)kRegPlanes * N + 5 * K) * sizeof(float); }
 };
 
 // One CTA's tile whose origin is (x0, y0).
@@ -46,6 +48,7 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   float* const sQY = sm + rQY * N;
   float* const sQZ = sm + rQZ * N;
   float* const sQW = sm + rQW * N;
+  float* const sSch = sm + kRegPlanes * N;
 
   const long n = (long)h * w;
   const long base = (long)(y0 - 2 * K) * w + (x0 - 2 * K);
@@ -58,6 +61,12 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   // first, the state (which that launch writes) only after griddepcontrol.wait
   // (a no-op for an ordinary launch).
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  const int k = niter < K ? niter : K;
+  if (threadIdx.x < 5 * k) {  // this launch's step sizes and dual-step scales
+    const int t = threadIdx.x / 5, c = threadIdx.x - 5 * t;
+    sSch[threadIdx.x] = c < 3 ? reinterpret_cast<const float*>(sched + it0 + t)[c]
+                              : reinterpret_cast<const float*>(kc.dscale + it0 + t)[c - 3];
+  }
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int e = threadIdx.x + j * NT;
@@ -87,8 +96,7 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   live = __syncthreads_or(live);
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
   if (!live) {
-    const int k0 = niter < K ? niter : K;
-    for (int s = 0; s < (TRACE ? k0 : 1); ++s) {
+    for (int s = 0; s < (TRACE ? k : 1); ++s) {
       const long ro = (long)s * rec_stride;
 #pragma unroll
       for (int j = 0; j < J; ++j) {
@@ -123,11 +131,10 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   }
   __syncthreads();
 
-  const int k = niter < K ? niter : K;
   for (int s = 1; s <= k; ++s) {
-    const float3 ss = sched[it0 + s - 1];  // (sigma, tau, mu)
-    const float2 dsc = kc.dscale[it0 + s - 1];  // alpha1 sigma / etaP, alpha0 sigma / etaQ
-    const float scaleP = dsc.x, scaleQ = dsc.y;
+    const float* const sc = sSch + 5 * (s - 1);
+    const float3 ss = make_float3(sc[0], sc[1], sc[2]);  // (sigma, tau, mu)
+    const float scaleP = sc[3], scaleQ = sc[4];           // alpha1 sigma / etaP, alpha0 sigma / etaQ
     {  // dual step on [lo, hiX) x [lo, hiY)
       const int lo = 2 * K - 2 * (k - s) - 1;
       const int hiX = 2 * K + TX + (k - s), hiY = 2 * K + TY + (k - s);
