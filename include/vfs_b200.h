@@ -112,6 +112,16 @@ VFS_API int vfs_upsampling_vector_field(float* out_hw2, uint64_t src_tex, const 
 /* triangulateRays, Python/vfs.py:535-559 (t: 3 floats, host memory) */
 VFS_API int vfs_triangulate_rays(float* out_hw3, const float* rays_hw3, const float* rays_other_hw3, const float* t,
                          const uint8_t* mask, size_t mask_pitch, int h, int w, void* stream);
+/* Option beside triangulateRays (same arguments and masked output (0, 0, -1)):
+ * least-squares triangulation that uses all three components of t.  The
+ * reference's formula (Python/vfs.cu:728-734) uses only t.x and t.z and is
+ * ill-conditioned when the baseline is mostly along y or z.  Same convention
+ * (the other camera sees X at X + t); the result is the point on the
+ * reference ray closest to the other camera's ray,
+ * lambda * r, lambda = ((-t) x r_o) . (r x r_o) / |r x r_o|^2. */
+VFS_API int vfs_triangulate_rays_lsq(float* out_hw3, const float* rays_hw3, const float* rays_other_hw3,
+                                     const float* t, const uint8_t* mask, size_t mask_pitch, int h, int w,
+                                     void* stream);
 
 /* ---- equidistant camera (Python/equidistant_cam.py, Python/template_cam.cu) */
 /* getRays, Python/equidistant_cam.py:72-92 */
@@ -158,6 +168,9 @@ VFS_API int vfs_plan_solve(VfsPlan* plan, const uint8_t* img_ref, const uint8_t*
 /* triangulate_flow, Python/vfs.py:535-559, for the flow of the last solve */
 VFS_API int vfs_plan_triangulate(VfsPlan* plan, float f, float u0, float v0, const float* t, float* xyz_out_hw3,
                          void* stream);
+/* vfs_plan_triangulate with the least-squares rule of vfs_triangulate_rays_lsq */
+VFS_API int vfs_plan_triangulate_lsq(VfsPlan* plan, float f, float u0, float v0, const float* t,
+                                     float* xyz_out_hw3, void* stream);
 /* The per-iteration step sizes (sigma, tau, mu) the solve uses, as the
  * reference's host loop computes them (Python/vfs.py:494-515, NumPy >= 2
  * scalar rules); out3 receives 3*n floats.  Host-only, no GPU needed. */
@@ -198,6 +211,9 @@ VFS_API int vfs_batch_solve(VfsBatch* batch, const uint8_t* const* img_refs, con
                             float* const* warps_out_hw2, void* stream);
 VFS_API int vfs_batch_triangulate(VfsBatch* batch, int i, float f, float u0, float v0, const float* t,
                                   float* xyz_out_hw3, void* stream);
+/* vfs_batch_triangulate with the least-squares rule of vfs_triangulate_rays_lsq */
+VFS_API int vfs_batch_triangulate_lsq(VfsBatch* batch, int i, float f, float u0, float v0, const float* t,
+                                      float* xyz_out_hw3, void* stream);
 /* per-level TGV kernel of the batched launches (a 1xx register-owned variant) */
 VFS_API int vfs_batch_set_level_variant(VfsBatch* batch, int level, int variant);
 VFS_API int vfs_batch_set_graph(VfsBatch* batch, int enable);
@@ -262,7 +278,7 @@ VFS_API int vfs_grad_forward(VfsGradPlan* plan, const float* img_ref, const floa
 VFS_API int vfs_grad_backward(VfsGradPlan* plan, const float* g_depth, float* g_ref, float* g_other,
                               double* g_scalars, void* stream);
 /* Backward kernels: fused_reverse selects how an iteration is reversed:
- * 11..18 (default 11) several iterations per launch, cotangent state on chip
+ * 11..19 (default 11) several iterations per launch, cotangent state on chip
  * (11: 2 iterations, 24x16 tiles; 12: 2, 16x16; 13: 3, 16x16; 14: 4, 16x8;
  * 15: 2, 8x8; 16: 4, 8x8; 17: 3, 24x12; 18: 2, 32x12), 1..5 one iteration per launch in one tiled kernel
  * (1: 32x16; 2: 32x8; 3: 64x8; 4: 32x32; 5: 28x16), 0 three gather kernels.

@@ -384,6 +384,24 @@ def triangulate_rays(rays, rays_o, t, M):
     return out
 
 
+def triangulate_rays_lsq(rays, rays_o, t, M):
+    """Least-squares option beside ``triangulateRays`` (Python/vfs.cu:707-745),
+    with no reference counterpart: the point on the reference ray closest to
+    the other camera's ray ``-t + s * rays_o`` (the reference's convention,
+    the other camera sees X at X + t), using all three components of t."""
+    r = np.asarray(rays, F64)
+    o = np.asarray(rays_o, F64)
+    tt = np.asarray(t, F64).reshape(3)
+    n = np.cross(r, o)
+    m = np.cross(np.broadcast_to(-tt, o.shape), o)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        lam = np.sum(m * n, -1) / np.sum(n * n, -1)
+    out = lam[..., None] * r
+    msk = np.asarray(M) != 0
+    out[~msk] = (0.0, 0.0, -1.0)
+    return out
+
+
 # ---------------------------------------------------------------- camera
 class EquidistantCam64:
     """``EquidistantCamera`` (Python/equidistant_cam.cuh:32-59) and the
@@ -545,9 +563,10 @@ class VFS64:
         self.warpUV = warp
         return warp
 
-    def triangulate_flow(self, camera, translation):
-        """Python/vfs.py:535-559."""
+    def triangulate_flow(self, camera, translation, method="reference"):
+        """Python/vfs.py:535-559 (``method="lsq"``: ``triangulate_rays_lsq``)."""
         sz = self.warpUV.shape[:2]
         rays = camera.get_rays(sz)
         rays_o = camera.unproject(get_grid_zero(sz) + self.warpUV)
-        return triangulate_rays(rays, rays_o, np.asarray(translation, F64).reshape(3), self.masks[0])
+        tri = triangulate_rays_lsq if method == "lsq" else triangulate_rays
+        return tri(rays, rays_o, np.asarray(translation, F64).reshape(3), self.masks[0])

@@ -16,6 +16,7 @@ import numpy as np
 import pytest
 
 from helpers import bench_params, default_params, pair
+from vfs_b200.synthetic import make_pair
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "vfs_b200.h")
@@ -109,6 +110,57 @@ def test_synthetic_pairs_are_deterministic():
     assert np.array_equal(a.img_ref, b.img_ref) and np.array_equal(a.img_other, b.img_other)
     assert not np.array_equal(a.img_ref, c.img_ref)
     assert a.img_ref.dtype == np.uint8 and a.mask.max() == 255
+
+
+def test_synthetic_rotation_is_undone_by_the_calibration_field():
+    """A rotated second view, warped by the reference's calibration field
+    (cvf = project(R X) - grid, Python/vector_field.py:50-54, applied as in
+    Python/vfs.py:150-153), matches the unrotated second view of the same scene."""
+    from oracle.np64 import vfs64 as V
+    from vfs_b200.synthetic import rotation_xyz
+    n = 96
+    R = rotation_xyz(0.03, -0.04, 0.02)
+    a = pair(n, t=(0.1, 0.02, 0.0), seed=3)
+    b = make_pair(n, (0.1, 0.02, 0.0), seed=3, R=R)
+    assert np.array_equal(a.img_ref, b.img_ref) and np.array_equal(b.R, R)
+    cam = V.EquidistantCam64(b.intrinsics)
+    tvf_a, cvf_a = V.get_vector_fields(V.get_grid_zero((n, n)), cam, cam, a.R, a.t, 1)
+    tvf_b, cvf_b = V.get_vector_fields(V.get_grid_zero((n, n)), cam, cam, b.R, b.t, 1)
+    assert np.abs(cvf_a).max() < 1e-9 and np.abs(cvf_b).max() > 1.0
+    assert np.array_equal(tvf_a, tvf_b)  # the translation field ignores R
+    calib = V.warping_image(b.img_other.astype(np.float64), cvf_b)
+    inner = a.mask != 0
+    diff = np.abs(calib - a.img_other)[inner]
+    unrelated = np.abs(b.img_other.astype(np.float64) - a.img_other)[inner]
+    assert diff.mean() < 4.0 and unrelated.mean() > 4 * diff.mean(), (diff.mean(), unrelated.mean())
+
+
+def test_lsq_triangulation_recovers_points_for_any_baseline():
+    """The least-squares option recovers exact points for every baseline
+    direction; the reference's x-only formula (Python/vfs.cu:728-734) is exact
+    only while t.x dominates and fails for a vertical baseline."""
+    from oracle.np64 import vfs64 as V
+    rng = np.random.default_rng(0)
+    n = 2000
+    d = rng.normal(size=(n, 3))
+    d[:, 2] = np.abs(d[:, 2]) + 0.2
+    X = d / np.linalg.norm(d, axis=1, keepdims=True) * rng.uniform(1, 10, (n, 1))
+    M = np.ones(n, np.uint8)
+    unit = lambda v: v / np.linalg.norm(v, axis=-1, keepdims=True)
+    for t in [(0.1, 0.0, 0.0), (0.12, 0.01, 0.0), (0.0, 0.1, 0.0), (0.03, -0.05, 0.08)]:
+        t = np.asarray(t)
+        r, o = unit(X), unit(X + t)
+        got = V.triangulate_rays_lsq(r, o, t, M)
+        assert np.allclose(got, X, rtol=1e-9, atol=0), t
+        ref = V.triangulate_rays(r, o, t, M)
+        if t[0] != 0:
+            assert np.allclose(ref, X, rtol=1e-6, atol=0), t
+        else:
+            assert not np.allclose(ref, X, rtol=1e-2, atol=0, equal_nan=False)
+    # masked pixels take the reference's (0, 0, -1)
+    M[:3] = 0
+    out = V.triangulate_rays_lsq(unit(X), unit(X + 0.1), np.full(3, 0.1), M)
+    assert np.array_equal(out[:3], np.tile([0.0, 0.0, -1.0], (3, 1)))
 
 
 # ---------------------------------------------------------------- oracle vs golden

@@ -287,3 +287,53 @@ def test_autotuned_levels_bit_exact(ref_mod):
     for c in (162, 192, CLUSTER):
         o.set_level_variants([c] * prm.nLevel)
         assert_bits_equal(rw, _np(o.solve_stereo(p.img_ref, p.img_other)), f"warpUV with {c} everywhere")
+
+
+def test_solve_bit_exact_rotated_pair(ref_mod):
+    """A second view rotated by R (X_other = R (X + t)): the calibration warp by
+    cvf (Python/vfs.py:150-153) is no longer a near-identity, and the solve
+    still matches the reference's kernels bit for bit."""
+    from vfs_b200.synthetic import make_pair, rotation_xyz
+    h, w = 96, 128
+    p = make_pair(w, (0.1, 0.03, 0.01), seed=8, n_level=3, height=h, R=rotation_xyz(0.02, -0.03, 0.015))
+    prm = bench_params(h, w, n_level=3, n_warp=3, n_iter=13)
+    (rw, rxyz), outs, o, cam = _solve_pair(ref_mod, prm, p, variants=((4, False), (134, False)))
+    _, cvf = _fields(p)
+    assert np.abs(cvf).max() > 1.0
+    for v, (ow, oxyz) in outs.items():
+        assert_bits_equal(rw, ow, f"warpUV {v}")
+        assert_bits_equal(rxyz, oxyz, f"xyz {v}")
+
+
+def test_lsq_triangulation_against_float64(ref_mod):
+    """triangulate_flow(method="lsq") (fused plan kernel and the ray-by-ray
+    entry point) against the float64 oracle's least-squares triangulation of
+    the same flow.  Where the parallax angle exceeds 1 mrad the float32 result
+    is within 1e-3 relative of float64; the two GPU paths agree bit for bit."""
+    from oracle.np64 import vfs64 as V
+    h, w = 96, 128
+    t = (0.05, 0.1, 0.02)  # mostly vertical: the reference formula is ill-conditioned here
+    p = pair(w, height=h, t=t, seed=5, n_level=3)
+    prm = bench_params(h, w, n_level=3, n_warp=3, n_iter=13)
+    _, o = _both(ref_mod, prm, p)
+    from vfs_b200.equidistant_cam import EquidistantCam
+    cam = EquidistantCam(p.intrinsics)
+    cam.setup_module()
+    flow = _np(o.solve_stereo(p.img_ref, p.img_other))
+    fused = _np(o.triangulate_flow(cam, p.t, method="lsq"))
+    steps = _np(o.solve_stereo_steps(p.img_ref, p.img_other))
+    assert_bits_equal(flow, steps, "flow (plan vs per-step path)")
+    raywise = _np(o.triangulate_flow(cam, p.t, method="lsq"))
+    assert_bits_equal(fused, raywise, "lsq xyz (fused vs ray-by-ray)")
+    cam64 = V.EquidistantCam64(p.intrinsics)
+    rays = cam64.get_rays((h, w))
+    rays_o = cam64.unproject(V.get_grid_zero((h, w)) + flow.astype(np.float64))
+    want = V.triangulate_rays_lsq(rays, rays_o, np.asarray(t, np.float64), p.mask)
+    m = p.mask != 0
+    assert np.array_equal(fused[~m], np.tile(np.float32([0, 0, -1]), (np.count_nonzero(~m), 1)))
+    parallax = np.linalg.norm(np.cross(rays, rays_o), axis=-1)
+    sel = m & (parallax > 1e-3) & np.isfinite(want).all(-1)
+    assert sel.sum() > 0.5 * m.sum()
+    rel = np.abs(fused[sel, 2] - want[sel, 2]) / np.abs(want[sel, 2])
+    assert rel.max() < 1e-3, (rel.max(), np.median(rel))
+    assert np.median(rel) < 1e-5

@@ -306,6 +306,12 @@ int vfs_batch_triangulate(VfsBatch* bt, int i, float f, float u0, float v0, cons
   return vfs_plan_triangulate(bt->plans[i], f, u0, v0, t, xyz_out, stream);
 }
 
+int vfs_batch_triangulate_lsq(VfsBatch* bt, int i, float f, float u0, float v0, const float* t, float* xyz_out,
+                              void* stream) {
+  if (!bt || i < 0 || i >= bt->n) return fail(VFS_ERR_ARG, "pair index out of range");
+  return vfs_plan_triangulate_lsq(bt->plans[i], f, u0, v0, t, xyz_out, stream);
+}
+
 int vfs_batch_stats(VfsBatch* bt, VfsSolveStats* out) {
   if (!bt || !out) return fail(VFS_ERR_ARG, "NULL argument");
   memset(out, 0, sizeof(*out));

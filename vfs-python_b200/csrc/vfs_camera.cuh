@@ -42,4 +42,26 @@ __device__ __forceinline__ float3 triangulate_px(float3 rr, float3 ro, float tx,
   return make_float3(ZRef * xyRef.x, ZRef * xyRef.y, ZRef);
 }
 
+// Least-squares triangulation along the reference ray, using all three
+// components of t (an option beside triangulate_px, which uses only t.x and
+// t.z, Python/vfs.cu:728-734, and is ill-conditioned when t is mostly along
+// y or z).  Same convention as the reference: the other camera sees X at
+// X + t, so its centre sits at -t and its ray is -t + s*ro.  The result is
+// the point lambda*rr on the reference ray closest to that ray:
+//   lambda = ((-t) x ro) . (rr x ro) / |rr x ro|^2.
+// The cross products keep the small parallax angle accurate in float32 (a
+// dot-product form would cancel in 1 - cos^2).  Parallel rays (epipole,
+// infinite depth) divide by zero, as the reference formula does.
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return make_float3(fmaf(a.y, b.z, -a.z * b.y), fmaf(a.z, b.x, -a.x * b.z), fmaf(a.x, b.y, -a.y * b.x));
+}
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+
+__device__ __forceinline__ float3 triangulate_lsq_px(float3 rr, float3 ro, float tx, float ty, float tz) {
+  const float3 n = cross3(rr, ro);
+  const float3 m = cross3(make_float3(-tx, -ty, -tz), ro);
+  const float lam = dot3(m, n) / dot3(n, n);
+  return make_float3(lam * rr.x, lam * rr.y, lam * rr.z);
+}
+
 }  // namespace vfs

@@ -256,6 +256,16 @@ int vfs_triangulate_rays(float* out, const float* rays, const float* rays_o, con
   return VFS_OK;
 }
 
+int vfs_triangulate_rays_lsq(float* out, const float* rays, const float* rays_o, const float* t, const uint8_t* mask,
+                             size_t mp, int h, int w, void* s) {
+  VFS_NONNULL(out, rays, rays_o, t, mask);
+  VFS_TRY(check_hw(h, w));
+  VFS_TRY_CUDA(launch_triangulate((float3*)out, (const float3*)rays, (const float3*)rays_o, t[0], t[1], t[2],
+                                  mplane(mask, mp, w), h, w, S(s), true),
+               "triangulateRays (least squares)");
+  return VFS_OK;
+}
+
 int vfs_cam_get_rays(float* out, float f, float u0, float v0, int h, int w, void* s) {
   VFS_NONNULL(out);
   VFS_TRY(check_hw(h, w));

@@ -1423,6 +1423,8 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 }
 
 // Blocked reverse configurations: id -> (iterations per launch, tile, threads).
+// One CTA per SM (registers and shared memory): 19 covers a 200^2 level
+// with 140 tiles, one wave on the 148 SMs, where 17 needs 153.
 #define VFS_REVB_SHAPES(X) \
   X(11, 2, 24, 16, 736)    \
   X(12, 2, 16, 16, 576)    \
@@ -1431,7 +1433,8 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   X(15, 2, 8, 8, 256)      \
   X(16, 4, 8, 8, 512)      \
   X(17, 3, 24, 12, 800)    \
-  X(18, 2, 32, 12, 768)
+  X(18, 2, 32, 12, 768)    \
+  X(19, 3, 20, 15, 800)
 
 // pdl: may start as a programmatic dependent of the previous launch (only
 // when that launch wrote none of the recorded states this one reads before

@@ -249,15 +249,24 @@ __global__ void k_mask_code(Plane<uint8_t> code, Plane<const uint8_t> mask, int 
   code.at(X, Y) = mask_code(mask, X, Y, h, w);
 }
 
+// LSQ: least-squares triangulation along the reference ray (all of t)
+// instead of the reference's x-only formula.
+template <bool LSQ>
+__device__ __forceinline__ float3 triangulate_any(float3 rr, float3 ro, float tx, float ty, float tz) {
+  return LSQ ? triangulate_lsq_px(rr, ro, tx, ty, tz) : triangulate_px(rr, ro, tx, tz);
+}
+
+template <bool LSQ>
 __global__ void k_triangulate(float3* out, const float3* __restrict__ rays, const float3* __restrict__ rays_o,
                               float tx, float ty, float tz, Plane<const uint8_t> mask, int h, int w) {
   VFS_PIXEL_PROLOGUE
   const long i = (long)Y * w + X;
-  out[i] = mask_at(mask, X, Y, h, w) ? triangulate_px(rays[i], rays_o[i], tx, tz) : make_float3(0, 0, -1);
+  out[i] = mask_at(mask, X, Y, h, w) ? triangulate_any<LSQ>(rays[i], rays_o[i], tx, ty, tz) : make_float3(0, 0, -1);
 }
 
 // Python/vfs.py:535-559 in one pass: getRays at the pixel, getXYZFromUV at
 // pixel + flow (float32 add, as `uv + self.warpUV`), then triangulateRays.
+template <bool LSQ>
 __global__ void k_triangulate_flow(float3* out, Plane<const float2> warp, Cam cam, float tx, float ty, float tz,
                                    Plane<const uint8_t> mask, int h, int w) {
   VFS_PIXEL_PROLOGUE
@@ -269,7 +278,7 @@ __global__ void k_triangulate_flow(float3* out, Plane<const float2> warp, Cam ca
   const float2 d = warp.at(X, Y);
   const float3 rr = cam_unproject(cam, make_float2((float)X, (float)Y));
   const float3 ro = cam_unproject(cam, make_float2((float)X + d.x, (float)Y + d.y));
-  out[i] = triangulate_px(rr, ro, tx, tz);
+  out[i] = triangulate_any<LSQ>(rr, ro, tx, ty, tz);
 }
 
 __global__ void k_get_rays(float3* out, Cam cam, int h, int w) {
@@ -424,12 +433,14 @@ cudaError_t launch_mask_code(Plane<uint8_t> code, Plane<const uint8_t> mask, int
   VFS_LAUNCH(k_mask_code, h, w, s, code, mask, h, w);
 }
 cudaError_t launch_triangulate(float3* out, const float3* rays, const float3* rays_o, float tx, float ty, float tz,
-                               Plane<const uint8_t> mask, int h, int w, cudaStream_t s) {
-  VFS_LAUNCH(k_triangulate, h, w, s, out, rays, rays_o, tx, ty, tz, mask, h, w);
+                               Plane<const uint8_t> mask, int h, int w, cudaStream_t s, bool lsq) {
+  if (lsq) VFS_LAUNCH(k_triangulate<true>, h, w, s, out, rays, rays_o, tx, ty, tz, mask, h, w);
+  VFS_LAUNCH(k_triangulate<false>, h, w, s, out, rays, rays_o, tx, ty, tz, mask, h, w);
 }
 cudaError_t launch_triangulate_flow(float3* out, Plane<const float2> warp, Cam cam, float tx, float ty, float tz,
-                                    Plane<const uint8_t> mask, int h, int w, cudaStream_t s) {
-  VFS_LAUNCH(k_triangulate_flow, h, w, s, out, warp, cam, tx, ty, tz, mask, h, w);
+                                    Plane<const uint8_t> mask, int h, int w, cudaStream_t s, bool lsq) {
+  if (lsq) VFS_LAUNCH(k_triangulate_flow<true>, h, w, s, out, warp, cam, tx, ty, tz, mask, h, w);
+  VFS_LAUNCH(k_triangulate_flow<false>, h, w, s, out, warp, cam, tx, ty, tz, mask, h, w);
 }
 cudaError_t launch_get_rays(float3* out, Cam cam, int h, int w, cudaStream_t s) {
   VFS_LAUNCH(k_get_rays, h, w, s, out, cam, h, w);

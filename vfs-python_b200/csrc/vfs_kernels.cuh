@@ -88,10 +88,12 @@ cudaError_t launch_upsample1(Plane<float> out, cudaTextureObject_t src, float sc
 cudaError_t launch_upsample2(Plane<float2> out, cudaTextureObject_t src, float scale, int h, int w, cudaStream_t s);
 cudaError_t launch_mask_flow(Plane<float2> warp, Plane<const uint8_t> mask, int h, int w, cudaStream_t s);
 cudaError_t launch_mask_code(Plane<uint8_t> code, Plane<const uint8_t> mask, int h, int w, cudaStream_t s);
+// lsq: least-squares triangulation along the reference ray instead of the
+// reference's x-only formula (triangulate_lsq_px, vfs_camera.cuh)
 cudaError_t launch_triangulate(float3* out, const float3* rays, const float3* rays_o, float tx, float ty, float tz,
-                               Plane<const uint8_t> mask, int h, int w, cudaStream_t s);
+                               Plane<const uint8_t> mask, int h, int w, cudaStream_t s, bool lsq = false);
 cudaError_t launch_triangulate_flow(float3* out, Plane<const float2> warp, Cam cam, float tx, float ty, float tz,
-                                    Plane<const uint8_t> mask, int h, int w, cudaStream_t s);
+                                    Plane<const uint8_t> mask, int h, int w, cudaStream_t s, bool lsq = false);
 cudaError_t launch_get_rays(float3* out, Cam cam, int h, int w, cudaStream_t s);
 cudaError_t launch_get_thetas(float3* out, const float3* rays, int h, int w, cudaStream_t s);
 cudaError_t launch_project(float2* out, const float3* xyz, Cam cam, int h, int w, cudaStream_t s);

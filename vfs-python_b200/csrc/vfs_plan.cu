@@ -578,15 +578,25 @@ int vfs_plan_stats(VfsPlan* pl, VfsSolveStats* out) {
   return VFS_OK;
 }
 
-int vfs_plan_triangulate(VfsPlan* pl, float f, float u0, float v0f, const float* t, float* xyz_out, void* stream) {
+static int plan_triangulate(VfsPlan* pl, float f, float u0, float v0f, const float* t, float* xyz_out, void* stream,
+                            bool lsq) {
   if (!pl || !t || !xyz_out) return fail(VFS_ERR_ARG, "NULL argument");
   if (!pl->solved) return fail(VFS_ERR_STATE, "triangulate needs a solve first");
   auto& v0 = pl->lv[0];
   VFS_TRY_CUDA(launch_triangulate_flow(reinterpret_cast<float3*>(xyz_out), {pl->warp[0].ptr, pl->warp[0].pitch},
                                        Cam{f, u0, v0f}, t[0], t[1], t[2], {v0.mask.ptr, v0.mask.pitch}, v0.h, v0.w,
-                                       (cudaStream_t)stream),
+                                       (cudaStream_t)stream, lsq),
                "triangulate");
   return VFS_OK;
+}
+
+int vfs_plan_triangulate(VfsPlan* pl, float f, float u0, float v0f, const float* t, float* xyz_out, void* stream) {
+  return plan_triangulate(pl, f, u0, v0f, t, xyz_out, stream, false);
+}
+
+int vfs_plan_triangulate_lsq(VfsPlan* pl, float f, float u0, float v0f, const float* t, float* xyz_out,
+                             void* stream) {
+  return plan_triangulate(pl, f, u0, v0f, t, xyz_out, stream, true);
 }
 
 }  // extern "C"

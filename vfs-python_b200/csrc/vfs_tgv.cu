@@ -266,6 +266,10 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
 
 // Compiled variants: id -> (implementation, iterations per launch, tile).
 // Ids below 100 keep all state in shared memory; ids 1xx are register-owned.
+// Ids 22x have tiles sized so that a pyramid level of side S = 12 T covers
+// at most 144 tiles, one per SM of the 148: the 1024-thread kernels hold one
+// CTA per SM, so 169 tiles of a power-of-two side would need a second wave
+// (e.g. 34x34 at 400^2, 17x17 at 200^2, 9x9 at 100^2, 27x27 at 320^2).
 #define VFS_TGV_VARIANTS(X)          \
   X(1, block, 1, 32, 16, 256)        \
   X(2, block, 2, 32, 32, 512)        \
@@ -305,7 +309,14 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   X(214, reg, 8, 8, 8, 1024)         \
   X(215, reg, 6, 12, 12, 928)        \
   X(216, reg, 5, 16, 16, 1024)       \
-  X(217, reg, 6, 14, 14, 1024)
+  X(217, reg, 6, 14, 14, 1024)       \
+  X(220, reg, 3, 34, 34, 1024)       \
+  X(221, reg, 3, 36, 36, 1024)       \
+  X(222, reg, 4, 17, 17, 864)        \
+  X(223, reg, 5, 17, 17, 1024)       \
+  X(224, reg, 6, 9, 9, 736)          \
+  X(225, reg, 4, 11, 11, 544)        \
+  X(226, reg, 4, 27, 27, 1024)
 
 // Register-owned variants also compiled in recording form (every
 // iteration's state written out), for the reverse mode's recomputation.
@@ -314,7 +325,10 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   X(134, 4, 32, 32, 1024)         \
   X(207, 4, 8, 8, 416)            \
   X(212, 4, 20, 20, 1024)         \
-  X(216, 5, 16, 16, 1024)
+  X(216, 5, 16, 16, 1024)         \
+  X(220, 3, 34, 34, 1024)         \
+  X(222, 4, 17, 17, 864)          \
+  X(224, 6, 9, 9, 736)
 
 }  // namespace
 

@@ -79,6 +79,7 @@ _SIGS = {
     "vfs_upsampling_vector_field1": [_P, _U64, _PRM, _I, _I, _P],
     "vfs_upsampling_vector_field": [_P, _U64, _PRM, _I, _I, _P],
     "vfs_triangulate_rays": [_P, _P, _P, _P, _P, _SZ, _I, _I, _P],
+    "vfs_triangulate_rays_lsq": [_P, _P, _P, _P, _P, _SZ, _I, _I, _P],
     "vfs_cam_get_rays": [_P, _F, _F, _F, _I, _I, _P],
     "vfs_cam_get_uvs": [_P, _P, _F, _F, _F, _I, _I, _P],
     "vfs_cam_get_xyzs": [_P, _P, _F, _F, _F, _I, _I, _P],
@@ -93,6 +94,7 @@ _SIGS = {
     "vfs_plan_set_vector_fields": [_P, _P, _P, _P],
     "vfs_plan_solve": [_P, _P, _P, _P, _P],
     "vfs_plan_triangulate": [_P, _F, _F, _F, _P, _P, _P],
+    "vfs_plan_triangulate_lsq": [_P, _F, _F, _F, _P, _P, _P],
     "vfs_plan_set_tgv_variant": [_P, _I],
     "vfs_plan_set_graph": [_P, _I],
     "vfs_tgv_variants": [_P, _I, _P],
@@ -103,6 +105,7 @@ _SIGS = {
     "vfs_batch_set_pair": [_P, _I, _P, _SZ, _P, _P, _P],
     "vfs_batch_solve": [_P, _P, _P, _P, _P],
     "vfs_batch_triangulate": [_P, _I, _F, _F, _F, _P, _P, _P],
+    "vfs_batch_triangulate_lsq": [_P, _I, _F, _F, _F, _P, _P, _P],
     "vfs_batch_set_level_variant": [_P, _I, _I],
     "vfs_batch_set_graph": [_P, _I],
     "vfs_batch_set_timing": [_P, _I],

@@ -76,11 +76,14 @@ class VFSBatch:
         self._inputs = (refs, oths)
         return outs
 
-    def triangulate(self, i, camera, translation):
+    def triangulate(self, i, camera, translation, method="reference"):
+        """Depth points of pair i (VFS.triangulate_flow's two methods)."""
+        if method not in ("reference", "lsq"):
+            raise ValueError(f"triangulation method {method!r}: use 'reference' or 'lsq'")
         t = np.asarray(translation, dtype=np.float32).reshape(-1)
         out = torch.empty((*self.sizes[i], 3), dtype=torch.float32, device="cuda")
         f, u0, v0 = camera._k()
-        call("vfs_batch_triangulate", self._batch, int(i), f, u0, v0, (ctypes.c_float * 3)(*t.tolist()),
+        call("vfs_batch_triangulate" + ("_lsq" if method == "lsq" else ""), self._batch, int(i), f, u0, v0, (ctypes.c_float * 3)(*t.tolist()),
              out.data_ptr(), stream())
         return out
 

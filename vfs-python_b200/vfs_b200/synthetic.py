@@ -3,11 +3,13 @@
 A scene is a range field over the reference camera's pixels (a tilted plane
 plus eight Gaussian bumps, clipped to [1, 10] m) textured with 4-octave value
 noise in [0, 255] that is evaluated analytically at continuous coordinates.
-The second view sees every reference point ``X`` at ``X + t`` (no rotation),
-the convention of the reference's vector-field generator and triangulation
-(Python/vector_field.py:36-44, Python/vfs.cu:728-734).  For each pixel of the
-second image the reference pixel that lands there is found by fixed-point
-iteration on the flow, so the second image needs no resampling.
+The second view sees every reference point ``X`` at ``R (X + t)``, the
+convention of the reference's vector-field generator and triangulation
+(Python/vector_field.py:36-54, Python/vfs.cu:728-734): the calibration field
+``project(R X) - grid`` undoes R, and the translation field and triangulation
+work on ``X + t``.  R defaults to the identity.  For each pixel of the second
+image the reference pixel that lands there (after undoing R) is found by
+fixed-point iteration on the flow, so the second image needs no resampling.
 
 The mask is the reference driver's circle (Python/main_equidistant.py:52-53)
 with margin ``max(10, 2**(nLevel-1))`` pixels.
@@ -110,11 +112,22 @@ def circle_mask(height: int, width: int, margin: int) -> np.ndarray:
     return mask
 
 
-def make_pair(size: int, t, seed: int = 0, n_level: int = 4, height: int | None = None) -> StereoPair:
-    """One seeded pair at ``size`` x ``size`` (or ``height`` x ``size``)."""
+def rotation_xyz(rx: float, ry: float, rz: float) -> np.ndarray:
+    """Rotation matrix Rz(rz) @ Ry(ry) @ Rx(rx), angles in radians."""
+    cx, sx, cy, sy, cz, sz = np.cos(rx), np.sin(rx), np.cos(ry), np.sin(ry), np.cos(rz), np.sin(rz)
+    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    return Rz @ Ry @ Rx
+
+
+def make_pair(size: int, t, seed: int = 0, n_level: int = 4, height: int | None = None, R=None) -> StereoPair:
+    """One seeded pair at ``size`` x ``size`` (or ``height`` x ``size``);
+    ``R`` (3x3) rotates the second view, X_other = R (X + t)."""
     W = int(size)
     H = int(height if height is not None else size)
     t = np.asarray(t, np.float64).reshape(3)
+    R = np.eye(3) if R is None else np.asarray(R, np.float64).reshape(3, 3)
     rng = np.random.default_rng(seed)
     f, cx, cy = equidistant_intrinsics(W, H)
     noise = _ValueNoise(rng, W, H)
@@ -129,11 +142,18 @@ def make_pair(size: int, t, seed: int = 0, n_level: int = 4, height: int | None 
         uv = _project(X, f, cx, cy)
         return uv[..., 0] - px, uv[..., 1] - py
 
-    p1x, p1y = xx.copy(), yy.copy()
+    # target of the fixed point: the second view's pixel with R undone
+    if np.array_equal(R, np.eye(3)):
+        gx, gy = xx, yy
+    else:
+        d = _unproject(np.stack([xx, yy], -1), f, cx, cy) @ R  # rows R^T d
+        g = _project(d, f, cx, cy)
+        gx, gy = g[..., 0], g[..., 1]
+    p1x, p1y = gx.copy(), gy.copy()
     for _ in range(30):
         fx, fy = flow(p1x, p1y)
-        p1x = 0.5 * p1x + 0.5 * (xx - fx)
-        p1y = 0.5 * p1y + 0.5 * (yy - fy)
+        p1x = 0.5 * p1x + 0.5 * (gx - fx)
+        p1y = 0.5 * p1y + 0.5 * (gy - fy)
     img_other = noise(p1x, p1y)
 
     ray = _unproject(np.stack([xx, yy], -1), f, cx, cy)
@@ -141,5 +161,5 @@ def make_pair(size: int, t, seed: int = 0, n_level: int = 4, height: int | None 
     margin = max(10, 2 ** (n_level - 1))
     mask = circle_mask(H, W, margin)
     q = lambda a: np.clip(np.round(a), 0, 255).astype(np.uint8)
-    return StereoPair(q(img_ref), q(img_other), mask, (f, cx, cy), np.eye(3), t.reshape(3, 1), depth, seed,
+    return StereoPair(q(img_ref), q(img_other), mask, (f, cx, cy), R, t.reshape(3, 1), depth, seed,
                       {"margin": margin})

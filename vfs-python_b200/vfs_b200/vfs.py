@@ -397,7 +397,15 @@ class VFS:
         return warpUV_ref
 
     # ---- Python/vfs.py:535-559
-    def triangulate_flow(self, camera, translation):
+    def triangulate_flow(self, camera, translation, method="reference"):
+        """Rays of the grid and of grid + flow, triangulated with the
+        translation.  ``method="reference"`` is the reference's formula
+        (x components, t.x and t.z only); ``method="lsq"`` is the
+        least-squares point on the reference ray closest to the other ray,
+        which uses all of t (for baselines mostly along y or z)."""
+        if method not in ("reference", "lsq"):
+            raise ValueError(f"triangulation method {method!r}: use 'reference' or 'lsq'")
+        sfx = "_lsq" if method == "lsq" else ""
         t = np.asarray(translation, dtype=np.float32).reshape(-1)
         assert t.size == 3
         h, w = self.warpUV.shape[:2]
@@ -406,7 +414,7 @@ class VFS:
         if self._plan is not None and getattr(self, "_fused_flow", None) is self.warpUV:
             # getRays + getXYZFromUV + triangulateRays in one kernel on the
             # plan's copy of the flow
-            call("vfs_plan_triangulate", self._plan, float(np.float32(camera.f)), float(np.float32(camera.u0)),
+            call("vfs_plan_triangulate" + sfx, self._plan, float(np.float32(camera.f)), float(np.float32(camera.u0)),
                  float(np.float32(camera.v0)), tt, out.data_ptr(), stream())
             return out
         # rays of the grid and of grid + flow, then triangulateRays
@@ -414,7 +422,7 @@ class VFS:
         from .vector_field import get_grid_zero
         rays_other = camera.get_XYZs(get_grid_zero((h, w)) + self.warpUV)
         m = self.masks_to[0]
-        call("vfs_triangulate_rays", out.data_ptr(), rays.data_ptr(), rays_other.data_ptr(), tt, m.data_ptr,
+        call("vfs_triangulate_rays" + sfx, out.data_ptr(), rays.data_ptr(), rays_other.data_ptr(), tt, m.data_ptr,
              m.pitch, h, w, stream())
         return out
 
