@@ -280,7 +280,8 @@ VFS_API int vfs_grad_backward(VfsGradPlan* plan, const float* g_depth, float* g_
 /* Backward kernels: fused_reverse selects how an iteration is reversed:
  * 11..19 (default 11) several iterations per launch, cotangent state on chip
  * (11: 2 iterations, 24x16 tiles; 12: 2, 16x16; 13: 3, 16x16; 14: 4, 16x8;
- * 15: 2, 8x8; 16: 4, 8x8; 17: 3, 24x12; 18: 2, 32x12), 1..5 one iteration per launch in one tiled kernel
+ * 15: 2, 8x8; 16: 4, 8x8; 17: 3, 24x12; 18: 2, 32x12; 19: 3, 20x15), 1..5 one iteration per launch in
+ * one tiled kernel
  * (1: 32x16; 2: 32x8; 3: 64x8; 4: 32x32; 5: 28x16), 0 three gather kernels.
  * trace_variant selects the TGV variant that recomputes checkpoint intervals
  * (0: automatic, -1: one iteration per launch).  With ckpt_every 1 the
@@ -289,6 +290,10 @@ VFS_API int vfs_grad_set_options(VfsGradPlan* plan, int fused_reverse, int trace
 /* Reverse-step kernel form for one level (0: the plan's, from
  * vfs_grad_set_options; default 11).  Level 0 is the finest. */
 VFS_API int vfs_grad_set_level_form(VfsGradPlan* plan, int level, int form);
+/* Triangulation rule of the depth map and of its reverse: 0 the reference's
+ * (Python/vfs.cu:728-734, default), 1 least squares along the reference ray
+ * (vfs_triangulate_rays_lsq).  A forward must follow a change. */
+VFS_API int vfs_grad_set_triangulation(VfsGradPlan* plan, int lsq);
 /* Event timing of the reverse TGV launches of each backward (off by default).
  * vfs_grad_stats (after synchronising) fills tgv_ms, tgv_alg_bytes (241 per
  * pixel and reversed iteration: state before 40, p and q after 24, cotangent

@@ -304,16 +304,74 @@ def triangulate_vjp(cam, warp, t, M, g_depth):
     return np.stack([gZ_xo * dxo_du, gZ_xo * dxo_dv], -1), g_t
 
 
+def _unproject_and_jac(cam, uv):
+    """Unit ray of ``EquidistantCamera::unproject`` (Python/equidistant_cam.cuh:46-59)
+    at uv and its Jacobian d ray / d (u, v), shape (..., 3, 2).  With
+    x, y relative to the principal point, rho = |(x, y)|, theta = rho / f and
+    S = sin(theta) / rho: ray = (S x, S y, cos theta)."""
+    x = uv[..., 0] - cam.u0
+    y = uv[..., 1] - cam.v0
+    rho = np.hypot(x, y)
+    th = rho / cam.f
+    small = th < 1e-3
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rs = np.where(small, 1.0, rho)
+        S = np.where(small, (1 - th * th / 6 + th ** 4 / 120) / cam.f, np.sin(th) / rs)
+        Sp = np.where(small, (-1.0 / 3 + th * th / 30) / cam.f ** 3,  # (dS/drho) / rho
+                      (rho * np.cos(th) / cam.f - np.sin(th)) / rs ** 3)
+    ray = np.stack([S * x, S * y, np.cos(th)], -1)
+    J = np.empty(uv.shape[:-1] + (3, 2))
+    J[..., 0, 0] = S + x * x * Sp
+    J[..., 0, 1] = J[..., 1, 0] = x * y * Sp
+    J[..., 1, 1] = S + y * y * Sp
+    J[..., 2, 0] = -S * x / cam.f
+    J[..., 2, 1] = -S * y / cam.f
+    return ray, J
+
+
+def triangulate_lsq_vjp(cam, warp, t, M, g_depth):
+    """Adjoint of the depth map of ``triangulate_flow(method="lsq")``
+    (vfs64.triangulate_rays_lsq; no reference counterpart): (g_warp, g_t).
+    depth = lambda r_z with lambda = (m . n) / (n . n), n = r x o,
+    m = (-t) x o, o = unproject(grid + warp)."""
+    t = np.asarray(t, F64).reshape(3)
+    H, W = warp.shape[:2]
+    grid = V.get_grid_zero((H, W))
+    rr = cam.unproject(grid)
+    ro, J = _unproject_and_jac(cam, grid + warp)
+    msk = (np.asarray(M) != 0) & (g_depth != 0)
+    n = np.cross(rr, ro)
+    m = np.cross(np.broadcast_to(-t, ro.shape), ro)
+    nn = np.sum(n * n, -1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        lam = np.sum(m * n, -1) / nn
+        g_lam = np.where(msk, g_depth * rr[..., 2], 0.0)
+        gm = (g_lam / nn)[..., None] * n
+        gn = (g_lam / nn)[..., None] * (m - 2 * lam[..., None] * n)
+    gm = np.where(msk[..., None], gm, 0.0)
+    gn = np.where(msk[..., None], gn, 0.0)
+    # m = (-t) x o: d/d(-t) = o x gm, d/do = gm x (-t); n = r x o: d/do = gn x r
+    g_t = -np.sum(np.cross(ro, gm), axis=(0, 1))
+    g_o = np.cross(gm, np.broadcast_to(-t, ro.shape)) + np.cross(gn, rr)
+    g_warp = np.einsum("...i,...ij->...j", g_o, J)
+    return np.where(msk[..., None], g_warp, 0.0), g_t
+
+
 # ---------------------------------------------------------------- whole solve
 class Problem:
     """What stays fixed while the solve is differentiated: parameters (loop
-    counts, fScale, limitRange, timeStepLambda), camera, mask, ``t_scale``."""
+    counts, fScale, limitRange, timeStepLambda), camera, mask, ``t_scale``,
+    and the triangulation rule ("reference": Python/vfs.cu:728-734; "lsq":
+    least squares along the reference ray)."""
 
-    def __init__(self, prm, cam, mask, t_scale=1.0):
+    def __init__(self, prm, cam, mask, t_scale=1.0, triangulation="reference"):
         self.prm = prm
         self.cam = cam
         self.mask = np.asarray(mask, np.uint8)
         self.t_scale = float(t_scale)
+        if triangulation not in ("reference", "lsq"):
+            raise ValueError(triangulation)
+        self.triangulation = triangulation
 
 
 def _params(prob, theta):
@@ -386,7 +444,8 @@ def solve(prob, I0, I1, t, theta, mode="exact", tape=False):
             u = u_.copy()
             warp = V.upsampling(warp, *ss, prm.fScale, mode)
     warp = np.where((masks[0] != 0)[..., None], warp, 0.0)
-    depth = V.triangulate_rays(cam.get_rays((H, W)), cam.unproject(V.get_grid_zero((H, W)) + warp), t, masks[0])[..., 2]
+    tri = V.triangulate_rays_lsq if prob.triangulation == "lsq" else V.triangulate_rays
+    depth = tri(cam.get_rays((H, W)), cam.unproject(V.get_grid_zero((H, W)) + warp), t, masks[0])[..., 2]
     if not tape:
         return depth
     return depth, {"prm": prm, "t": t, "cvf": cvf, "I1": np.asarray(I1, F64), "sizes": sizes, "masks": masks,
@@ -400,7 +459,8 @@ def backward(prob, tp, g_depth):
     prm, sizes, masks = tp["prm"], tp["sizes"], tp["masks"]
     cam = prob.cam
     L = len(sizes)
-    g_warp, g_t = triangulate_vjp(cam, tp["warp"], tp["t"], masks[0], g_depth)
+    tri_vjp = triangulate_lsq_vjp if prob.triangulation == "lsq" else triangulate_vjp
+    g_warp, g_t = tri_vjp(cam, tp["warp"], tp["t"], masks[0], g_depth)
     g_warp = np.where((masks[0] != 0)[..., None], g_warp, 0.0)
     g_u = np.zeros(sizes[0])
     g_ub = np.zeros(sizes[0])

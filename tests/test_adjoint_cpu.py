@@ -124,22 +124,41 @@ def test_stage_vjps_match_finite_differences():
     _fd_check(tri, wp, lambda a, w: G.triangulate_vjp(cam, a, t, Mm, w)[0], rng, rtol=1e-5)
     _fd_check(lambda a: tri(wp, a), t, lambda a, w: G.triangulate_vjp(cam, wp, a, Mm, w)[1], rng)
 
+    def tri_lsq(a, tt=t):
+        z = V.triangulate_rays_lsq(cam.get_rays((48, 48)), cam.unproject(V.get_grid_zero((48, 48)) + a), tt,
+                                   Mm)[..., 2]
+        return np.where(Mm != 0, z, 0)
+    _fd_check(tri_lsq, wp, lambda a, w: G.triangulate_lsq_vjp(cam, a, t, Mm, w)[0], rng, rtol=1e-5)
+    _fd_check(lambda a: tri_lsq(wp, a), t, lambda a, w: G.triangulate_lsq_vjp(cam, wp, a, Mm, w)[1], rng)
+    # the unprojection Jacobian, including the series branch at the principal point
+    uv = np.concatenate([rng.uniform(0, 48, (40, 2)), cam.u0 + rng.normal(0, 1e-3, (8, 2)),
+                         np.array([[cam.u0, cam.v0]])])
+    ray, Jac = G._unproject_and_jac(cam, uv)
+    assert np.allclose(ray, cam.unproject(uv), rtol=0, atol=1e-15)
+    for j in range(2):
+        e = np.eye(2)[j] * 1e-6
+        fd = (cam.unproject(uv + e) - cam.unproject(uv - e)) / 2e-6
+        assert np.allclose(Jac[..., j], fd, rtol=0, atol=1e-8)
 
-def test_solve_vjp_matches_finite_differences():
+
+@pytest.mark.parametrize("triangulation", ["reference", "lsq"])
+def test_solve_vjp_matches_finite_differences(triangulation):
     """Whole coarse-to-fine solve, depth cotangent -> images, t, theta.
 
     The unrolled solve is piecewise smooth: median selection, the limitRange
     clamp, the shrink cases and the unit-ball projections switch inside a
     1e-4 stencil on this problem, so the float64 differences are taken at
-    h = 1e-8 along image directions and 1e-6 along t and theta, where they
-    have converged.
+    h = 1e-8 along image directions, 1e-7 along t and 1e-5 along theta, where
+    they have converged (along t.y, h = 1e-6 is still 6e-5..1e-4 off for both
+    triangulation rules, 1e-7 agrees to 3e-7; along theta the least-squares
+    depths carry more rounding noise, 3e-4 at h = 1e-6 against 4e-5 at 1e-5).
     """
     from oracle.np64 import grad64 as G
     from oracle.np64 import vfs64 as V
     from helpers import pair
     P = pair(48, t=(0.12, 0.01, 0.0), n_level=2)
     prm = bench_params(48, 48, n_level=2, n_warp=2, n_iter=6)
-    prob = G.Problem(prm, V.EquidistantCam64(P.intrinsics), P.mask)
+    prob = G.Problem(prm, V.EquidistantCam64(P.intrinsics), P.mask, triangulation=triangulation)
     nz = np.random.default_rng(9)     # continuous images: no exact ties in the median windows
     I0 = P.img_ref / 256.0 + nz.uniform(0, 1 / 256, (48, 48))
     I1 = P.img_other / 256.0 + nz.uniform(0, 1 / 256, (48, 48))
@@ -156,7 +175,7 @@ def test_solve_vjp_matches_finite_differences():
     checks += [(2, np.eye(3)[j], g["t"]) for j in range(3)]
     checks += [(3, np.eye(5)[j], g["theta"]) for j in range(5)]
     for i, d, gi in checks:
-        h = 1e-8 if i < 2 else 1e-6
+        h = {0: 1e-8, 1: 1e-8, 2: 1e-7, 3: 1e-5}[i]
         ap, am = list(base), list(base)
         ap[i] = base[i] + h * d
         am[i] = base[i] - h * d

@@ -11,8 +11,8 @@ from helpers import bench_params, pair
 pytestmark = pytest.mark.gpu
 
 
-def _problem(size=64, n_level=2, n_warp=3, n_iter=10, seed=0):
-    P = pair(size, t=(0.12, 0.01, 0.0), n_level=n_level, seed=seed)
+def _problem(size=64, n_level=2, n_warp=3, n_iter=10, seed=0, t=(0.12, 0.01, 0.0)):
+    P = pair(size, t=t, n_level=n_level, seed=seed)
     prm = bench_params(size, size, n_level=n_level, n_warp=n_warp, n_iter=n_iter)
     nz = np.random.default_rng(9)  # continuous images: no exact ties in the median windows
     I0 = (P.img_ref + nz.uniform(0, 1, P.img_ref.shape)).astype(np.float32)
@@ -20,16 +20,18 @@ def _problem(size=64, n_level=2, n_warp=3, n_iter=10, seed=0):
     return P, prm, I0, I1
 
 
-def _solver(P, prm, ckpt=4):
+def _solver(P, prm, ckpt=4, triangulation="reference"):
     from vfs_b200 import DepthSolver, EquidistantCam
-    return DepthSolver(prm, EquidistantCam(P.intrinsics), P.mask, t_scale=1.0, ckpt_every=ckpt)
+    return DepthSolver(prm, EquidistantCam(P.intrinsics), P.mask, t_scale=1.0, ckpt_every=ckpt,
+                       triangulation=triangulation)
 
 
 def _theta(prm):
     return np.array([prm.Lambda, prm.alpha0, prm.alpha1, prm.beta, prm.gamma])
 
 
-def test_grad_forward_is_the_plain_solve():
+@pytest.mark.parametrize("triangulation", ["reference", "lsq"])
+def test_grad_forward_is_the_plain_solve(triangulation):
     """The recording forward gives the drop-in solve's depth bit for bit."""
     from vfs_b200 import VFS, EquidistantCam
     from vfs_b200.vector_field import get_vector_fields, get_grid_zero
@@ -43,8 +45,8 @@ def test_grad_forward_is_the_plain_solve():
     v.create_mask_pyramid(P.mask)
     v.create_vector_field_pyramid(tvf, cvf)
     v.solve_stereo(P.img_ref, P.img_other)
-    want = v.triangulate_flow(cam, P.t)[..., 2].cpu().numpy()
-    s = _solver(P, prm, ckpt=7)
+    want = v.triangulate_flow(cam, P.t, method=triangulation)[..., 2].cpu().numpy()
+    s = _solver(P, prm, ckpt=7, triangulation=triangulation)
     got = s.forward_pass(torch.as_tensor(P.img_ref).float().cuda(), torch.as_tensor(P.img_other).float().cuda(),
                          torch.tensor(P.t.reshape(3)), torch.tensor(_theta(prm))).cpu().numpy()
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
@@ -63,20 +65,22 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
 
 
-def test_grad_matches_float64_reverse_mode():
+@pytest.mark.parametrize("triangulation,t", [("reference", (0.12, 0.01, 0.0)), ("lsq", (0.06, 0.1, 0.02))])
+def test_grad_matches_float64_reverse_mode(triangulation, t):
     """Same inputs, same cotangent: CUDA float32 gradients against the float64
-    reverse mode run along the texture-quantised forward ("tex8")."""
+    reverse mode run along the texture-quantised forward ("tex8"), for both
+    triangulation rules (the least-squares one on a mostly vertical baseline)."""
     from oracle.np64 import grad64 as G
     from oracle.np64 import vfs64 as V
-    P, prm, I0, I1 = _problem()
+    P, prm, I0, I1 = _problem(t=t)
     t = P.t.reshape(3).astype(np.float64)
     theta = _theta(prm)
-    s = _solver(P, prm, ckpt=4)
+    s = _solver(P, prm, ckpt=4, triangulation=triangulation)
     d, g_ref, g_other, g_t, g_th = _gpu_grads(s, I0, I1, t, theta, np.zeros(I0.shape))
     good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
     wts = np.where(good, np.random.default_rng(0).normal(0, 1, good.shape), 0.0)
     d, g_ref, g_other, g_t, g_th = _gpu_grads(s, I0, I1, t, theta, wts)
-    prob = G.Problem(prm, V.EquidistantCam64(P.intrinsics), P.mask)
+    prob = G.Problem(prm, V.EquidistantCam64(P.intrinsics), P.mask, triangulation=triangulation)
     d64, tape = G.solve(prob, I0 / 256.0, I1 / 256.0, t, theta, mode="tex8", tape=True)
     g = G.backward(prob, tape, wts)
     # measured on a B200: 1.3e-4 (images), <= 2.5e-4 (scalars)

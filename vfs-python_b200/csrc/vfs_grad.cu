@@ -179,8 +179,10 @@ __global__ void k_g_scale(float* out, const float* __restrict__ in, float s, int
   if (inside) out[i] = in[i] * s;
 }
 
-// z of triangulate_flow's xyz (Python/vfs.py:535-559, Python/vfs.cu:707-745).
-__global__ void k_g_depth(float* depth, Plane<const float2> warp, Cam cam, float tx, float tz,
+// z of triangulate_flow's xyz (Python/vfs.py:535-559, Python/vfs.cu:707-745;
+// LSQ: the least-squares rule, triangulate_lsq_px).
+template <bool LSQ>
+__global__ void k_g_depth(float* depth, Plane<const float2> warp, Cam cam, float tx, float ty, float tz,
                           Plane<const uint8_t> mask, int h, int w) {
   GRAD_PIXEL
   if (!inside) return;
@@ -191,7 +193,7 @@ __global__ void k_g_depth(float* depth, Plane<const float2> warp, Cam cam, float
   const float2 d = warp.at(X, Y);
   const float3 rr = cam_unproject(cam, make_float2((float)X, (float)Y));
   const float3 ro = cam_unproject(cam, make_float2((float)X + d.x, (float)Y + d.y));
-  depth[i] = triangulate_px(rr, ro, tx, tz).z;
+  depth[i] = LSQ ? triangulate_lsq_px(rr, ro, tx, ty, tz).z : triangulate_px(rr, ro, tx, tz).z;
 }
 
 // ---------------------------------------------------------------- triangulation
@@ -229,6 +231,61 @@ __global__ void k_g_tri(const float* __restrict__ gdepth, Plane<const float2> wa
       gw = make_float2(gx * fmaf(x * x, Gpr, G), gx * x * y * Gpr);
       acc[0] = g / D;
       acc[2] = -g * xo / D;
+    }
+    gwarp[i] = gw;
+  }
+  block_sum_to<3>(acc, scal + G_T0);
+}
+
+// d depth / d flow and d depth / d t for the least-squares rule:
+// depth = lambda r_z, lambda = (m . n) / (n . n), n = r x o, m = (-t) x o,
+// o = unproject((X, Y) + flow).  With x, y relative to the principal point,
+// rho = |(x, y)|, theta = rho / f, S = sin(theta) / rho, o = (S x, S y,
+// cos theta) and d o / d(x, y) = [[S + x^2 S', x y S'], [x y S', S + y^2 S'],
+// [-S x / f, -S y / f]] with S' = (dS/drho) / rho (series below theta 0.05).
+__global__ void k_g_tri_lsq(const float* __restrict__ gdepth, Plane<const float2> warp, Cam cam, float tx, float ty,
+                            float tz, Plane<const uint8_t> mask, float2* gwarp, double* scal, int h, int w) {
+  GRAD_PIXEL
+  float acc[3] = {0.f, 0.f, 0.f};
+  if (inside) {
+    float2 gw = make_float2(0.f, 0.f);
+    const float g = gdepth[i];
+    if (mask.at(X, Y) != 0 && g != 0.f) {
+      const float2 d = warp.at(X, Y);
+      const float3 rr = cam_unproject(cam, make_float2((float)X, (float)Y));
+      const float2 uv = make_float2((float)X + d.x, (float)Y + d.y);
+      const float3 ro = cam_unproject(cam, uv);
+      const float3 mt = make_float3(-tx, -ty, -tz);
+      const float3 n = cross3(rr, ro), m = cross3(mt, ro);
+      const float inn = 1.f / dot3(n, n);
+      const float lam = dot3(m, n) * inn;
+      const float gl = g * rr.z * inn;
+      const float3 gm = make_float3(gl * n.x, gl * n.y, gl * n.z);
+      const float3 gn = make_float3(gl * (m.x - 2.f * lam * n.x), gl * (m.y - 2.f * lam * n.y),
+                                    gl * (m.z - 2.f * lam * n.z));
+      const float3 gt = cross3(gm, ro);  // -(o x gm)
+      const float3 a = cross3(gm, mt), b = cross3(gn, rr);
+      const float3 go = make_float3(a.x + b.x, a.y + b.y, a.z + b.z);
+      const float x = uv.x - cam.u0, y = uv.y - cam.v0;
+      const float rho = hypotf(x, y);
+      const float th = rho / cam.f;
+      float S, Sp;
+      if (th < 0.05f) {
+        const float t2 = th * th;
+        S = (1.f - t2 * (1.f / 6.f - t2 * (1.f / 120.f))) / cam.f;
+        Sp = (-1.f / 3.f + t2 * (1.f / 30.f - t2 * (1.f / 840.f))) / (cam.f * cam.f * cam.f);
+      } else {
+        float sn, cs;
+        sincosf(th, &sn, &cs);
+        S = sn / rho;
+        Sp = (rho * cs / cam.f - sn) / (rho * rho * rho);
+      }
+      const float jxy = x * y * Sp;
+      gw.x = go.x * fmaf(x * x, Sp, S) + go.y * jxy - go.z * S * x / cam.f;
+      gw.y = go.x * jxy + go.y * fmaf(y * y, Sp, S) - go.z * S * y / cam.f;
+      acc[0] = gt.x;
+      acc[1] = gt.y;
+      acc[2] = gt.z;
     }
     gwarp[i] = gw;
   }
@@ -1773,6 +1830,7 @@ struct VfsGradPlan {
   int tev_used = 0;
   int level_form[32] = {0};  // per level: 0 = fused_reverse
   int trace_variant = 0;  // 0: the level's forward variant if it records, else 134
+  bool tri_lsq = false;   // least-squares triangulation (vfs_grad_set_triangulation)
 };
 
 namespace {
@@ -2012,8 +2070,11 @@ int grad_forward(VfsGradPlan* gp, const float* img_ref, const float* img_other, 
     VFS_TRY(plan_level_end(pl, &c, s, &nk));
   }
   VFS_TRY(plan_finish(pl, s, &nk));
-  k_g_depth<<<g2d(v0.h, v0.w), kGB, 0, s>>>(depth, {pl->warp[0].ptr, pl->warp[0].pitch}, gp->cam, (float)gp->t[0],
-                                             (float)gp->t[2], {v0.mask.ptr, v0.mask.pitch}, v0.h, v0.w);
+  {
+    auto kern = gp->tri_lsq ? k_g_depth<true> : k_g_depth<false>;
+    kern<<<g2d(v0.h, v0.w), kGB, 0, s>>>(depth, {pl->warp[0].ptr, pl->warp[0].pitch}, gp->cam, (float)gp->t[0],
+                                         (float)gp->t[1], (float)gp->t[2], {v0.mask.ptr, v0.mask.pitch}, v0.h, v0.w);
+  }
   VFS_TRY_CUDA(cudaGetLastError(), "depth");
   pl->solved = true;
   return VFS_OK;
@@ -2063,9 +2124,14 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
   int cb = 0;  // which of the gu/gub/gwarp pairs holds the current level
   VFS_TRY_CUDA(zero(gp->gu[cb], n0 * 4, s), "memset");
   VFS_TRY_CUDA(zero(gp->gub[cb], n0 * 4, s), "memset");
-  k_g_tri<<<g2d(v0.h, v0.w), kGB, 0, s>>>(gdepth, {pl->warp[0].ptr, pl->warp[0].pitch}, gp->cam, (float)gp->t[0],
-                                           (float)gp->t[2], {v0.mask.ptr, v0.mask.pitch}, gp->gwarp[cb], gp->scal,
-                                           v0.h, v0.w);
+  if (gp->tri_lsq)
+    k_g_tri_lsq<<<g2d(v0.h, v0.w), kGB, 0, s>>>(gdepth, {pl->warp[0].ptr, pl->warp[0].pitch}, gp->cam,
+                                                 (float)gp->t[0], (float)gp->t[1], (float)gp->t[2],
+                                                 {v0.mask.ptr, v0.mask.pitch}, gp->gwarp[cb], gp->scal, v0.h, v0.w);
+  else
+    k_g_tri<<<g2d(v0.h, v0.w), kGB, 0, s>>>(gdepth, {pl->warp[0].ptr, pl->warp[0].pitch}, gp->cam, (float)gp->t[0],
+                                             (float)gp->t[2], {v0.mask.ptr, v0.mask.pitch}, gp->gwarp[cb], gp->scal,
+                                             v0.h, v0.w);
   VFS_TRY_CUDA(cudaGetLastError(), "triangulate backward");
   for (int l = 0; l < L; ++l) {
     auto& v = pl->lv[l];
@@ -2353,6 +2419,14 @@ int vfs_grad_set_level_form(VfsGradPlan* gp, int level, int form) {
   if (form != 0 && !rev_shape_ok(form) && rev_block_iters(form) == 0)
     return fail(VFS_ERR_ARG, "unknown reverse kernel form");
   gp->level_form[level] = form;
+  return VFS_OK;
+}
+
+int vfs_grad_set_triangulation(VfsGradPlan* gp, int lsq) {
+  if (!gp) return fail(VFS_ERR_ARG, "plan is NULL");
+  if (lsq != 0 && lsq != 1) return fail(VFS_ERR_ARG, "triangulation: 0 (reference) or 1 (least squares)");
+  gp->tri_lsq = lsq == 1;
+  gp->recorded = false;  // the recorded depth came from the other rule
   return VFS_OK;
 }
 

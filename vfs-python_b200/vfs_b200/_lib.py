@@ -125,6 +125,7 @@ _SIGS = {
     "vfs_grad_backward": [_P, _P, _P, _P, _P, _P],
     "vfs_grad_set_options": [_P, _I, _I],
     "vfs_grad_set_level_form": [_P, _I, _I],
+    "vfs_grad_set_triangulation": [_P, _I],
     "vfs_grad_set_timing": [_P, _I],
     "vfs_grad_stats": [_P, ctypes.POINTER(VfsSolveStats)],
 }

@@ -21,6 +21,7 @@ of each level for both passes.
 
     solver = DepthSolver(param, camera, mask)
     depth = solver(img_ref, img_other, t, theta)       # autograd-aware
+    # DepthSolver(..., triangulation="lsq") uses all three components of t
     loss = (depth - gt).abs()[mask != 0].mean(); loss.backward()
 """
 from __future__ import annotations
@@ -37,7 +38,13 @@ THETA = ("Lambda", "alpha0", "alpha1", "beta", "gamma")
 
 
 class DepthSolver:
-    def __init__(self, param, camera, mask, t_scale: float = 1.0, ckpt_every: int = 10, level_variants=None):
+    def __init__(self, param, camera, mask, t_scale: float = 1.0, ckpt_every: int = 10, level_variants=None,
+                 triangulation: str = "reference"):
+        """``triangulation``: "reference" (the reference's x-only formula) or
+        "lsq" (least squares along the reference ray, all of t; the choice for
+        baselines with large y or z components)."""
+        if triangulation not in ("reference", "lsq"):
+            raise ValueError(f"triangulation {triangulation!r}: use 'reference' or 'lsq'")
         self.param = param
         self.prm = _lib.VfsParams.from_param_bag(param)
         self.ckpt_every = int(ckpt_every)
@@ -56,6 +63,8 @@ class DepthSolver:
         if tuple(self._mask.shape) != self.shape:
             raise AssertionError(f"mask shape {tuple(self._mask.shape)} != {self.shape}")
         self._plan = _lib.lib().vfs_grad_plan(self._gp)
+        self.triangulation = triangulation
+        call("vfs_grad_set_triangulation", self._gp, int(triangulation == "lsq"))
         call("vfs_plan_set_mask", self._plan, self._mask.data_ptr(), self.shape[1], stream())
         for lvl, var in enumerate(level_variants or []):
             if var:
