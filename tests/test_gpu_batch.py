@@ -48,9 +48,10 @@ def test_batched_solve_matches_single_pair_and_reference(gpu):
             v.create_vector_field_pyramid(tvf, cvf)
             single = v.solve_stereo(p.img_ref, p.img_other).cpu().numpy()
             assert np.array_equal(_bits(single), _bits(warps[i])), f"pair {i} (graph {graph})"
-            xb = batch.triangulate(i, cam, p.t).cpu().numpy()
-            xs = v.triangulate_flow(cam, p.t).cpu().numpy()
-            assert np.array_equal(_bits(xb), _bits(xs)), f"pair {i} xyz"
+            for method in ("reference", "lsq"):
+                xb = batch.triangulate(i, cam, p.t, method=method).cpu().numpy()
+                xs = v.triangulate_flow(cam, p.t, method=method).cpu().numpy()
+                assert np.array_equal(_bits(xb), _bits(xs)), f"pair {i} xyz ({method})"
     # one pair against the reference's own kernels
     r = refpath.RefVFS(bench_params(*sizes[1], n_level=3, n_warp=2, n_iter=11), "bench")
     r.compute_pyramid_sizes()

@@ -337,3 +337,22 @@ def test_lsq_triangulation_against_float64(ref_mod):
     rel = np.abs(fused[sel, 2] - want[sel, 2]) / np.abs(want[sel, 2])
     assert rel.max() < 1e-3, (rel.max(), np.median(rel))
     assert np.median(rel) < 1e-5
+
+
+@pytest.mark.parametrize("h,w,n_level,n_warp,n_iter,mask_kind", [
+    (17, 23, 2, 2, 5, "circle"),    # smaller than every tile
+    (61, 53, 3, 2, 7, "circle"),    # odd, ragged sizes
+    (48, 40, 1, 1, 1, "circle"),    # one level, one warp, one iteration
+    (64, 64, 3, 2, 6, "zero"),      # every pixel masked: every tile skips its iterations
+])
+def test_solve_bit_exact_edge_cases(ref_mod, h, w, n_level, n_warp, n_iter, mask_kind):
+    p = pair(w, height=h, seed=11, n_level=max(n_level, 2))
+    prm = bench_params(h, w, n_level=n_level, n_warp=n_warp, n_iter=n_iter)
+    mask = np.zeros((h, w), np.uint8) if mask_kind == "zero" else p.mask
+    variants = ((4, False), (134, False), (220, False), (222, False), (224, False), (134, True))
+    (rw, rxyz), outs, _, _ = _solve_pair(ref_mod, prm, p, mask=mask, variants=variants)
+    if mask_kind == "zero":
+        assert not rw.any()
+    for v, (ow, oxyz) in outs.items():
+        assert_bits_equal(rw, ow, f"warpUV {v}")
+        assert_bits_equal(rxyz, oxyz, f"xyz {v}")
