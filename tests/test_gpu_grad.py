@@ -78,10 +78,18 @@ def test_grad_matches_float64_reverse_mode(triangulation, t):
     s = _solver(P, prm, ckpt=4, triangulation=triangulation)
     d, g_ref, g_other, g_t, g_th = _gpu_grads(s, I0, I1, t, theta, np.zeros(I0.shape))
     good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
-    wts = np.where(good, np.random.default_rng(0).normal(0, 1, good.shape), 0.0)
-    d, g_ref, g_other, g_t, g_th = _gpu_grads(s, I0, I1, t, theta, wts)
     prob = G.Problem(prm, V.EquidistantCam64(P.intrinsics), P.mask, triangulation=triangulation)
     d64, tape = G.solve(prob, I0 / 256.0, I1 / 256.0, t, theta, mode="tex8", tape=True)
+    if triangulation == "lsq":
+        # this baseline puts the epipole inside the image; beside it the rays
+        # are nearly parallel (|r x o| ~ 2e-5), the depth gradient reaches 1e7
+        # and float32 ray rounding alone moves it by 1 %: leave parallax below
+        # 1 mrad out of the loss (40 of 1403 pixels here)
+        grid = V.get_grid_zero(P.mask.shape)
+        par = np.linalg.norm(np.cross(prob.cam.unproject(grid), prob.cam.unproject(grid + tape["warp"])), axis=-1)
+        good &= par > 1e-3
+    wts = np.where(good, np.random.default_rng(0).normal(0, 1, good.shape), 0.0)
+    d, g_ref, g_other, g_t, g_th = _gpu_grads(s, I0, I1, t, theta, wts)
     g = G.backward(prob, tape, wts)
     # measured on a B200: 1.3e-4 (images), <= 2.5e-4 (scalars)
     assert _rel(g_ref, g["I0"] / 256.0) < 2e-3
