@@ -258,7 +258,11 @@ def run_b200(args, n, rank, local):
     vfs.configure(iters_per_launch=args.iters_per_launch, use_graph=not args.no_graph, timing=True)
     ref_d = torch.as_tensor(pair.img_ref).cuda()
     oth_d = torch.as_tensor(pair.img_other).cuda()
-    level_choice = vfs.autotune(ref_d, oth_d) if not args.no_autotune else None
+    if args.level_variants:
+        level_choice = [int(v) for v in args.level_variants.split(",")]
+        vfs.set_level_variants(level_choice)
+    else:
+        level_choice = vfs.autotune(ref_d, oth_d) if not args.no_autotune else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
@@ -787,6 +791,8 @@ def main():
     ap.add_argument("--iters-per-launch", type=int, default=134)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--level-variants", default="",
+                    help="single: comma-separated TGV kernel per level, finest first (skips the autotuner)")
     ap.add_argument("--workload", default="single", choices=["single", "batched", "batched800", "grad", "learn"],
                     help="single: the 800x800 pair (default); batched: 32 uneven pairs in one batch; "
                          "batched800: --pairs 800x800 pairs in one batch; "

@@ -155,7 +155,7 @@ def test_backward_kernel_forms_agree():
     good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
     wts = np.where(good, np.random.default_rng(2).normal(0, 1, good.shape), 0.0) * 1e-3
     outs = []
-    forms = [(0, -1), (1, -1), (0, 0), (1, 0), (1, 124), (1, 216), (1, 220), (1, 222), (1, 224), (2, 0), (3, 0),
+    forms = [(0, -1), (1, -1), (0, 0), (1, 0), (1, 124), (1, 216), (1, 220), (1, 221), (1, 222), (1, 224), (2, 0), (3, 0),
              (4, 0), (5, 0)]
     forms += [(b, 0) for b in (11, 12, 13, 14, 15, 16, 17, 18, 19)]
     for fused, tv in forms:

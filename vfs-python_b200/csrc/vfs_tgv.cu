@@ -327,6 +327,7 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   X(212, 4, 20, 20, 1024)         \
   X(216, 5, 16, 16, 1024)         \
   X(220, 3, 34, 34, 1024)         \
+  X(221, 3, 36, 36, 1024)         \
   X(222, 4, 17, 17, 864)          \
   X(224, 6, 9, 9, 736)
 
