@@ -242,6 +242,10 @@ def cpu_baseline_sample(pair, p, budget_s=20.0):
                       f"iterations ({t_map:.0f} s per map)"}
 
 
+# ncu captures of the finest level's kernel, by TGV variant
+TRAFFIC_FILES = {221: "k_tgv_reg_36x36_800x800_ncu.json", 134: "k_tgv_reg_800x800_ncu.json"}
+
+
 def load_traffic(name="k_tgv_reg_800x800_ncu.json"):
     path = os.path.join(ROOT, "profiles", name)
     try:
@@ -329,7 +333,8 @@ def run_b200(args, n, rank, local):
     peak, peak_kind = measured_peak()
     achieved = tgv_bytes / (tgv_ms / 1e3) / 1e9 if tgv_ms > 0 else None
     traffic = None
-    tr = load_traffic()
+    fine = level_choice[0] if level_choice else args.iters_per_launch
+    tr = load_traffic(TRAFFIC_FILES[fine]) if fine in TRAFFIC_FILES else None
     if tr and tgv_launches:
         traffic = tr["dram_bytes_per_alg_byte"] * (tgv_bytes / tgv_launches)
     line = {
@@ -343,7 +348,7 @@ def run_b200(args, n, rank, local):
                    "tgv_kernel_per_level": level_choice, "cuda_graph": not args.no_graph,
                    "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "parallelism": f"dp{n} (independent pairs)"},
-        "roofline": {"bound": "hbm", "kernel": "k_tgv_block (fused TGV iterations)",
+        "roofline": {"bound": "hbm", "kernel": f"k_tgv_reg (fused TGV iterations; finest level variant {fine})",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                      "traffic": traffic,
