@@ -423,7 +423,8 @@ def run_batched(args, n, rank, local):
         batch.set_pair(i, pp.mask, tvf, cvf)
     refs = [torch.as_tensor(pp.img_ref).cuda() for pp in pairs]
     oths = [torch.as_tensor(pp.img_other).cuda() for pp in pairs]
-    choice = batch.autotune(refs, oths) if not args.no_autotune else None
+    cands = [int(c) for c in args.batch_candidates.split(",")] if args.batch_candidates else None
+    choice = batch.autotune(refs, oths, candidates=cands) if not args.no_autotune else None
     batch.configure(use_graph=True, timing=True)
     for _ in range(args.warmup):
         batch.solve(refs, oths)
@@ -803,6 +804,8 @@ def main():
                          "batched800: --pairs 800x800 pairs in one batch; "
                          "grad: forward + backward of 8 pairs at 512x512; learn: 16 pairs at 1024x1024")
     ap.add_argument("--pairs", type=int, default=8, help="batched800: pairs per GPU")
+    ap.add_argument("--batch-candidates", default="",
+                    help="batched: comma-separated TGV variants the batch autotuner may choose from (default: all)")
     ap.add_argument("--ckpt", type=int, default=0,
                     help="grad/learn: TGV iterations between recorded states (0: the workload's default)")
     ap.add_argument("--lr", type=float, default=1e-3,

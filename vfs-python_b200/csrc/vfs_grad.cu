@@ -1481,7 +1481,9 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 
 // Blocked reverse configurations: id -> (iterations per launch, tile, threads).
 // One CTA per SM (registers and shared memory): 19 covers a 200^2 level
-// with 140 tiles, one wave on the 148 SMs, where 17 needs 153.
+// with 140 tiles, one wave on the 148 SMs, where 17 needs 153; 20 is the
+// widest tile whose window (36x23) fits one pixel per thread within the
+// register budget, recomputing 1.85 window pixels per tile pixel (11: 1.92).
 #define VFS_REVB_SHAPES(X) \
   X(11, 2, 24, 16, 736)    \
   X(12, 2, 16, 16, 576)    \
@@ -1491,7 +1493,8 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   X(16, 4, 8, 8, 512)      \
   X(17, 3, 24, 12, 800)    \
   X(18, 2, 32, 12, 768)    \
-  X(19, 3, 20, 15, 800)
+  X(19, 3, 20, 15, 800)    \
+  X(20, 2, 28, 16, 832)
 
 // pdl: may start as a programmatic dependent of the previous launch (only
 // when that launch wrote none of the recorded states this one reads before

@@ -75,7 +75,7 @@ class DepthSolver:
 
     def set_options(self, fused_reverse: int = 11, trace_variant: int = 0) -> None:
         """Backward kernel forms (see vfs_grad_set_options in vfs_b200.h): the
-        reverse-step kernel (11..19 several iterations per launch, 1..5 one
+        reverse-step kernel (11..20 several iterations per launch, 1..5 one
         tiled kernel per iteration, 0 three gather kernels) and the TGV variant
         recomputing checkpoint intervals (0 automatic, -1 one iteration per launch)."""
         call("vfs_grad_set_options", self._gp, int(fused_reverse), int(trace_variant))
@@ -87,7 +87,7 @@ class DepthSolver:
         self.level_forms = list(forms)
 
     def autotune(self, img_ref, img_other, t, theta=None, g_depth=None,
-                 forms=(11, 13, 18, 17, 19, 12, 15, 16, 14), fwd_variants=(134, 124, 212, 216, 207, 220, 221, 222, 224),
+                 forms=(11, 20, 13, 18, 17, 19, 12, 15, 16, 14), fwd_variants=(134, 124, 212, 216, 207, 220, 221, 222, 224),
                  repeats: int = 2):
         """Choose, per level, the recording forward's TGV kernel and then the
         reverse-step form, by timing whole passes (levels are independent, so
