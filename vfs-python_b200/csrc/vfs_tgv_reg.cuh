@@ -6,24 +6,63 @@
 // threshold and primal steps read them at the pixel only) and the per-warp
 // constants (tensor, eta, derivatives, mask code).  Values that neighbours
 // read go to shared memory: u_ and v_ (read at E/W/S/N by the dual step), tp
-// and q (read at W/N by the threshold and primal steps).  That is 9 floats of
-// shared memory per window pixel instead of 20, and J independent pixels per
-// thread for the scheduler to interleave.
+// and q (read at W/N by the threshold and primal steps).  Kernels whose
+// threads own one window pixel store them as records, (u_, v_x, v_y, -) and q
+// as float4 and tp as float2, so that one 16- or 8-byte shared-memory access
+// moves what a neighbour contributes (~4 % faster on the coarse levels);
+// kernels whose threads own two or more keep nine float planes, which need
+// fewer registers.  That is 9-10 floats of shared memory per window pixel
+// instead of 20, and J independent pixels per thread for the scheduler to
+// interleave.
 #pragma once
 
 namespace vfs {
 namespace {
-
-enum RegPlane { rUB, rVX, rVY, rTX, rTY, rQX, rQY, rQZ, rQW, kRegPlanes };
 
 template <int K, int TX, int TY>
 struct RegGeom {
   static constexpr int WX = TX + 3 * K;
   static constexpr int WY = TY + 3 * K;
   static constexpr int N = WX * WY;
-  // the planes, then (sigma, tau, mu, scaleP, scaleQ) of each of the
-  // launch's iterations
-  static constexpr size_t smem_bytes() { return ((size_t)kRegPlanes * N + 5 * K) * sizeof(float); }
+  // the state (RegSmem: 40 bytes per window pixel packed, 36 as planes),
+  // then (sigma, tau, mu, scaleP, scaleQ) of each of the launch's iterations
+  static constexpr size_t smem_bytes() { return (size_t)N * (16 + 16 + 8) + 5 * K * sizeof(float); }
+};
+
+// The shared-memory state of a tile, in one of two layouts with the same
+// values: PACKED keeps (u_, v_x, v_y, -) and q as float4 records and tp as a
+// float2, so a neighbour's contribution is one 16- or 8-byte access (fewer
+// shared-memory instructions); otherwise nine float planes, which need fewer
+// registers (the kernels whose threads own two or more window pixels would
+// spill with the records).  Both fit in RegGeom::smem_bytes().
+template <bool PACKED, int N>
+struct RegSmem {
+  float4* base;
+  __device__ __forceinline__ float* pl(int p) const { return reinterpret_cast<float*>(base) + p * N; }
+  __device__ __forceinline__ float4 uv(int i) const {
+    if constexpr (PACKED) return base[i];
+    else return make_float4(pl(0)[i], pl(1)[i], pl(2)[i], 0.f);
+  }
+  __device__ __forceinline__ void set_uv(int i, float4 v) const {
+    if constexpr (PACKED) base[i] = v;
+    else pl(0)[i] = v.x, pl(1)[i] = v.y, pl(2)[i] = v.z;
+  }
+  __device__ __forceinline__ float4 q(int i) const {
+    if constexpr (PACKED) return base[N + i];
+    else return make_float4(pl(3)[i], pl(4)[i], pl(5)[i], pl(6)[i]);
+  }
+  __device__ __forceinline__ void set_q(int i, float4 v) const {
+    if constexpr (PACKED) base[N + i] = v;
+    else pl(3)[i] = v.x, pl(4)[i] = v.y, pl(5)[i] = v.z, pl(6)[i] = v.w;
+  }
+  __device__ __forceinline__ float2 tp(int i) const {
+    if constexpr (PACKED) return reinterpret_cast<const float2*>(base + 2 * N)[i];
+    else return make_float2(pl(7)[i], pl(8)[i]);
+  }
+  __device__ __forceinline__ void set_tp(int i, float2 v) const {
+    if constexpr (PACKED) reinterpret_cast<float2*>(base + 2 * N)[i] = v;
+    else pl(7)[i] = v.x, pl(8)[i] = v.y;
+  }
 };
 
 // One CTA's tile whose origin is (x0, y0).
@@ -38,17 +77,8 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   using G = RegGeom<K, TX, TY>;
   constexpr int WX = G::WX, N = G::N, J = (N + NT - 1) / NT;
   extern __shared__ float4 smem_raw[];
-  float* const sm = reinterpret_cast<float*>(smem_raw);
-  float* const sUB = sm + rUB * N;
-  float* const sVX = sm + rVX * N;
-  float* const sVY = sm + rVY * N;
-  float* const sTX = sm + rTX * N;
-  float* const sTY = sm + rTY * N;
-  float* const sQX = sm + rQX * N;
-  float* const sQY = sm + rQY * N;
-  float* const sQZ = sm + rQZ * N;
-  float* const sQW = sm + rQW * N;
-  float* const sSch = sm + kRegPlanes * N;
+  const RegSmem<J == 1, N> S{smem_raw};
+  float* const sSch = reinterpret_cast<float*>(smem_raw) + 10 * N;  // after 40 N bytes
 
   const long n = (long)h * w;
   const long base = (long)(y0 - 2 * K) * w + (x0 - 2 * K);
@@ -120,13 +150,8 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     rpx[j] = ok ? in.px[f] : 0.f;
     rpy[j] = ok ? in.py[f] : 0.f;
     if (e < N) {
-      sUB[e] = ok ? in.ub[f] : 0.f;
-      sVX[e] = ok ? in.vbx[f] : 0.f;
-      sVY[e] = ok ? in.vby[f] : 0.f;
-      sQX[e] = ok ? in.qx[f] : 0.f;
-      sQY[e] = ok ? in.qy[f] : 0.f;
-      sQZ[e] = ok ? in.qz[f] : 0.f;
-      sQW[e] = ok ? in.qw[f] : 0.f;
+      S.set_uv(e, ok ? make_float4(in.ub[f], in.vbx[f], in.vby[f], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f));
+      S.set_q(e, ok ? make_float4(in.qx[f], in.qy[f], in.qz[f], in.qw[f]) : make_float4(0.f, 0.f, 0.f, 0.f));
     }
   }
   __syncthreads();
@@ -145,24 +170,20 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
         const uint8_t code = (uint8_t)rcode[j];
         if (!(code & kSelf)) {
           rpx[j] = rpy[j] = 0.f;
-          sTX[i] = sTY[i] = 0.f;
-          sQX[i] = sQY[i] = sQZ[i] = sQW[i] = 0.f;
+          S.set_tp(i, make_float2(0.f, 0.f));
+          S.set_q(i, make_float4(0.f, 0.f, 0.f, 0.f));
           continue;
         }
         float2 p = make_float2(rpx[j], rpy[j]), tp;
-        float4 q = make_float4(sQX[i], sQY[i], sQZ[i], sQW[i]);
-        dual_px(code, sUB[i], make_float2(sVX[i], sVY[i]), sUB[i + 1], make_float2(sVX[i + 1], sVY[i + 1]),
-                sUB[i - 1], make_float2(sVX[i - 1], sVY[i - 1]), sUB[i + WX], make_float2(sVX[i + WX], sVY[i + WX]),
-                sUB[i - WX], make_float2(sVX[i - WX], sVY[i - WX]), make_float3(ra[j], rb[j], rc[j]), scaleP,
+        float4 q = S.q(i);
+        const float4 c = S.uv(i), cE = S.uv(i + 1), cW = S.uv(i - 1), cS = S.uv(i + WX), cN = S.uv(i - WX);
+        dual_px(code, c.x, make_float2(c.y, c.z), cE.x, make_float2(cE.y, cE.z), cW.x, make_float2(cW.y, cW.z),
+                cS.x, make_float2(cS.y, cS.z), cN.x, make_float2(cN.y, cN.z), make_float3(ra[j], rb[j], rc[j]), scaleP,
                 scaleQ, &p, &tp, &q);
         rpx[j] = p.x;
         rpy[j] = p.y;
-        sTX[i] = tp.x;
-        sTY[i] = tp.y;
-        sQX[i] = q.x;
-        sQY[i] = q.y;
-        sQZ[i] = q.z;
-        sQW[i] = q.w;
+        S.set_tp(i, tp);
+        S.set_q(i, q);
       }
     }
     __syncthreads();
@@ -176,23 +197,22 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
         const uint8_t code = (uint8_t)rcode[j];
         if (!(code & kSelf)) {
           ru[j] = 0.f;
-          sUB[i] = sVX[i] = sVY[i] = 0.f;
+          S.set_uv(i, make_float4(0.f, 0.f, 0.f, 0.f));
           continue;
         }
-        const float ub = sUB[i];
-        const float un = threshold_px(code, ss.y, make_float2(sTX[i], sTY[i]), make_float2(sTX[i - 1], 0.f),
-                                      make_float2(0.f, sTY[i - WX]), ru[j], ub, make_float2(riu[j], riz[j]), rex[j],
+        const float4 c = S.uv(i);
+        const float ub = c.x;
+        const float un = threshold_px(code, ss.y, S.tp(i), make_float2(S.tp(i - 1).x, 0.f),
+                                      make_float2(0.f, S.tp(i - WX).y), ru[j], ub, make_float2(riu[j], riz[j]), rex[j],
                                       kc.lambda);
         float uo;
         float2 vo;
-        primal_px(code, ss.y, ss.z, make_float2(rpx[j], rpy[j]), make_float4(sQX[i], sQY[i], sQZ[i], sQW[i]),
-                  make_float4(sQX[i - 1], 0.f, 0.f, sQW[i - 1]), make_float4(0.f, sQY[i - WX], sQZ[i - WX], 0.f),
-                  un, ub, make_float2(sVX[i], sVY[i]), make_float3(ra[j], rb[j], rc[j]),
+        const float4 qW = S.q(i - 1), qN = S.q(i - WX);
+        primal_px(code, ss.y, ss.z, make_float2(rpx[j], rpy[j]), S.q(i), make_float4(qW.x, 0.f, 0.f, qW.w),
+                  make_float4(0.f, qN.y, qN.z, 0.f), un, ub, make_float2(c.y, c.z), make_float3(ra[j], rb[j], rc[j]),
                   make_float3(rex[j], rey[j], rez[j]), kc.alpha0, kc.alpha1, &uo, &vo);
         ru[j] = un;
-        sUB[i] = uo;
-        sVX[i] = vo.x;
-        sVY[i] = vo.y;
+        S.set_uv(i, make_float4(uo, vo.x, vo.y, 0.f));
       }
     }
     if constexpr (TRACE) {  // each thread writes the tile pixels it owns
@@ -205,16 +225,17 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
         if (X >= w || Y >= h) continue;
         const int i = threadIdx.x + j * NT;
         const long f = (long)Y * w + X + ro;
+        const float4 uv = S.uv(i), q = S.q(i);
         out.u[f] = ru[j];
-        out.ub[f] = sUB[i];
-        out.vbx[f] = sVX[i];
-        out.vby[f] = sVY[i];
+        out.ub[f] = uv.x;
+        out.vbx[f] = uv.y;
+        out.vby[f] = uv.z;
         out.px[f] = rpx[j];
         out.py[f] = rpy[j];
-        out.qx[f] = sQX[i];
-        out.qy[f] = sQY[i];
-        out.qz[f] = sQZ[i];
-        out.qw[f] = sQW[i];
+        out.qx[f] = q.x;
+        out.qy[f] = q.y;
+        out.qz[f] = q.z;
+        out.qw[f] = q.w;
       }
     }
     __syncthreads();
@@ -230,16 +251,17 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     if (X >= w || Y >= h) continue;
     const int i = threadIdx.x + j * NT;
     const long f = (long)Y * w + X;
+    const float4 uv = S.uv(i), q = S.q(i);
     out.u[f] = ru[j];
-    out.ub[f] = sUB[i];
-    out.vbx[f] = sVX[i];
-    out.vby[f] = sVY[i];
+    out.ub[f] = uv.x;
+    out.vbx[f] = uv.y;
+    out.vby[f] = uv.z;
     out.px[f] = rpx[j];
     out.py[f] = rpy[j];
-    out.qx[f] = sQX[i];
-    out.qy[f] = sQY[i];
-    out.qz[f] = sQZ[i];
-    out.qw[f] = sQW[i];
+    out.qx[f] = q.x;
+    out.qy[f] = q.y;
+    out.qz[f] = q.z;
+    out.qw[f] = q.w;
   }
   }
 }
