@@ -579,17 +579,24 @@ def _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid):
     return solver.backward_pass(g)
 
 
+# ncu captures of the reverse kernel, by reverse form
+REV_TRAFFIC_FILES = {20: "k_rev_block_28x16_800x800_ncu.json", 11: "k_rev_block_800x800_ncu.json"}
+
+
 def reverse_roofline(solver, run_once):
     """Live roofline of the reverse TGV launches: one extra forward + backward
-    with event timing around the reverse launches (outside any timed loop)."""
-    tr = load_traffic("k_rev_block_800x800_ncu.json")
+    with event timing around the reverse launches (outside any timed loop);
+    traffic from the capture of the finest level's reverse form."""
+    forms = getattr(solver, "level_forms", None) or [11]
+    tr = load_traffic(REV_TRAFFIC_FILES[forms[0]]) if forms[0] in REV_TRAFFIC_FILES else None
     solver.set_timing(True)
     run_once()
     st = solver.backward_stats()
     solver.set_timing(False)
     peak, kind = measured_peak()
     achieved = st["tgv_alg_bytes"] / (st["tgv_ms"] / 1e3) / 1e9 if st["tgv_ms"] > 0 else None
-    return {"bound": "hbm", "kernel": "k_rev_block (reverse TGV iterations)", "achieved": achieved, "peak": peak,
+    return {"bound": "hbm", "kernel": f"k_rev_block (reverse TGV iterations; finest level form {forms[0]})",
+            "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": kind,
             "alg_bytes_per_pixel_iteration": 241, "alg_bytes_per_launch": st["tgv_alg_bytes"] / max(st["tgv_launches"], 1),
             "avg_launch_us": 1e3 * st["tgv_ms"] / max(st["tgv_launches"], 1), "reverse_tgv_ms": st["tgv_ms"],
