@@ -270,6 +270,10 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
 // at most 144 tiles, one per SM of the 148: the 1024-thread kernels hold one
 // CTA per SM, so 169 tiles of a power-of-two side would need a second wave
 // (e.g. 34x34 at 400^2, 17x17 at 200^2, 9x9 at 100^2, 27x27 at 320^2).
+// 221 (36x36, 3 iterations, a 45x45 window, two pixels per thread) is the
+// largest square tile within 1024 x 2 window pixels: the least halo per tile
+// pixel, and 529 tiles fill four waves at 800^2 (the 32x32 tiles' 625 need
+// five).
 #define VFS_TGV_VARIANTS(X)          \
   X(1, block, 1, 32, 16, 256)        \
   X(2, block, 2, 32, 32, 512)        \
