@@ -112,6 +112,29 @@ def test_synthetic_pairs_are_deterministic():
     assert a.img_ref.dtype == np.uint8 and a.mask.max() == 255
 
 
+def test_least_squares_triangulation_arguments_are_checked_on_the_host(lib):
+    """The least-squares entry points and options validate their arguments
+    before any CUDA call."""
+    L = lib.lib()
+    t = (ctypes.c_float * 3)(0.1, 0.0, 0.0)
+    d = ctypes.c_void_p(16)
+    assert L.vfs_triangulate_rays_lsq(None, d, d, t, d, 8, 4, 4, None) == lib.VFS_ERR_ARG
+    assert L.vfs_triangulate_rays_lsq(d, d, d, None, d, 8, 4, 4, None) == lib.VFS_ERR_ARG
+    assert L.vfs_plan_triangulate_lsq(None, 1.0, 0.0, 0.0, t, d, None) == lib.VFS_ERR_ARG
+    assert L.vfs_batch_triangulate_lsq(None, 0, 1.0, 0.0, 0.0, t, d, None) == lib.VFS_ERR_ARG
+    assert L.vfs_grad_set_triangulation(None, 1) == lib.VFS_ERR_ARG
+    from vfs_b200 import DepthSolver
+    with pytest.raises(ValueError):
+        DepthSolver(bench_params(16, 16, n_level=1), (10.0, 8.0, 8.0), np.zeros((16, 16), np.uint8),
+                    triangulation="midpoint")
+    from vfs_b200.vfs import VFS
+    with pytest.raises(ValueError):
+        VFS.triangulate_flow(object(), None, (0.1, 0, 0), method="midpoint")
+    from vfs_b200.batch import VFSBatch
+    with pytest.raises(ValueError):
+        VFSBatch.triangulate(object(), 0, None, (0.1, 0, 0), method="midpoint")
+
+
 def test_synthetic_rotation_is_undone_by_the_calibration_field():
     """A rotated second view, warped by the reference's calibration field
     (cvf = project(R X) - grid, Python/vector_field.py:50-54, applied as in
