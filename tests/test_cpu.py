@@ -305,3 +305,21 @@ def test_grad_workspace_size_and_validation(lib):
     assert rc == lib.VFS_ERR_ARG  # focal length must be positive
     assert lib.lib().vfs_grad_set_options(None, 11, 0) == lib.VFS_ERR_ARG
     assert lib.lib().vfs_grad_backward(None, None, None, None, None, None) == lib.VFS_ERR_ARG
+
+
+def test_bench_algorithmic_bytes_and_profile_files():
+    """bench.py's roofline basis: 113 B per pixel-iteration, 60 per pixel-warp,
+    41 per pixel-level, summed over the pyramid (1.989e10 B per 512x512 map with
+    4 levels x 10 warps x 50 iterations; 9.688e10 B per 800x800 map with
+    5 x 10 x 100), and the ncu summaries it scales traffic from are present."""
+    import json
+    import bench
+    p = bench.params()
+    assert bench.alg_bytes_per_map(p) == 96878952500
+    p.width = p.height = 512
+    p.nLevel, p.nSolverIters = 4, 50
+    assert abs(bench.alg_bytes_per_map(p) - 1.989e10) < 1e7
+    for name in list(bench.TRAFFIC_FILES.values()) + list(bench.REV_TRAFFIC_FILES.values()):
+        d = json.load(open(os.path.join(ROOT, "profiles", name)))
+        assert 0 < d["dram_bytes_per_alg_byte"] < 1
+        assert abs(d["dram_bytes_per_alg_byte"] - (d["dram_read_bytes"] + d["dram_write_bytes"]) / d["alg_bytes"]) < 1e-3
