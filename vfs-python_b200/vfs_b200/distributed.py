@@ -3,7 +3,8 @@
 Pairs are independent, so a batch is split across ranks with no collective on
 the data path; the only collectives are a max of device times (measurement)
 and a sum of the few learned-parameter gradients (parameter learning).  The
-reference has no multi-GPU path (SURVEY: single GPU, default stream).
+reference has no multi-GPU path: it runs on one GPU, on the default stream, and
+synchronises after every launch (e.g. Python/vfs.py:107-113).
 """
 from __future__ import annotations
 
