@@ -637,7 +637,9 @@ def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None
         f_ms += e[0].elapsed_time(e[1])
         b_ms += e[1].elapsed_time(e[2])
     out = {"ms_fwd_bwd": (f_ms + b_ms) / steps, "ms_recording_forward": f_ms / steps, "ms_backward": b_ms / steps,
-           "ckpt_every": ckpt, "reverse_forms_per_level": forms, "workspace_gb": solver.workspace_bytes / 1e9,
+           "ckpt_every": ckpt, "reverse_forms_per_level": forms,
+           "recording_forward_variants": getattr(solver, "level_variants", None),
+           "workspace_gb": solver.workspace_bytes / 1e9,
            "roofline": reverse_roofline(solver, lambda: _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid))}
     if plain_ms:
         out["ratio_to_forward"] = out["ms_fwd_bwd"] / plain_ms
@@ -822,6 +824,9 @@ def main():
                     help="with --profile-case: one forward + backward at the finest level only, 1 warp, "
                          "8 TGV iterations, every state recorded, reverse form --reverse-form")
     ap.add_argument("--reverse-form", type=int, default=11)
+    ap.add_argument("--trace-variant", type=int, default=0,
+                    help="with --profile-grad: TGV variant of the recording forward, one with a recording "
+                         "form (0: the default, 134)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--profile-case", action="store_true",
@@ -841,7 +846,8 @@ def main():
         p.width = p.height = args.profile_size
         p.nLevel, p.nWarpIters, p.nSolverIters = 1, 1, 8
         pair = make_pair(args.profile_size, T, seed=0, n_level=N_LEVEL)
-        solver = DepthSolver(p, EquidistantCam(pair.intrinsics), pair.mask, ckpt_every=1)
+        solver = DepthSolver(p, EquidistantCam(pair.intrinsics), pair.mask, ckpt_every=1,
+                             level_variants=[args.trace_variant] if args.trace_variant else None)
         solver.set_options(args.reverse_form, 0)
         gt = torch.as_tensor(pair.depth).cuda()
         valid = torch.as_tensor(pair.mask != 0).cuda()
