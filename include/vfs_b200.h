@@ -231,8 +231,12 @@ VFS_API int vfs_batch_stats(VfsBatch* batch, VfsSolveStats* out);
  * vfs_plan_workspace_size) are rejected with VFS_ERR_WORKSPACE.  The first call
  * on a device (and the first after a parameter change) sets up a plan over the
  * scratch and uploads the step sizes with a synchronous copy, so make it
- * before any stream capture.  All calls on a device share the scratch: calls
- * whose GPU work overlaps race, so issue them on one stream or order them. */
+ * before any stream capture.  A call that changes the parameters first waits
+ * until the previous call's kernels on the device have finished (it blocks),
+ * so calls are safe back to back on one stream across parameter changes.  All
+ * calls on a device share the scratch: calls with the same parameters whose
+ * GPU work overlaps (different, unordered streams) race, so issue them on one
+ * stream or order them. */
 VFS_API size_t vfs_static_scratch_bytes(void);
 VFS_API int vfs_solve_stereo_static(const VfsParams* prm, const uint8_t* mask, size_t mask_pitch,
                                     const float* tvf_hw2, const float* cvf_hw2, const uint8_t* img_ref,

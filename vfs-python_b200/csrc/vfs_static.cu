@@ -17,11 +17,17 @@
 // parameter change) also uploads the step-size schedule with a synchronous
 // copy, so it must come before any stream capture.
 //
+// A rebuild blocks the calling thread: it first waits (on an event recorded
+// after every call's work) until the previous call's kernels on this device
+// have finished, whatever stream they ran on, because they still read the
+// old plan's texture objects and the schedule in the scratch.  So calls that
+// change the parameters are safe back to back on one stream, or on several.
+//
 // Every call shares the one array per device: a call overwrites what the
 // previous call left there, and everything a solve reads is recomputed or
-// cleared by that solve.  Calls whose GPU work overlaps (on different
-// streams, or from threads that do not order their streams) race on the
-// array; issue them on one stream or order them.
+// cleared by that solve.  Calls with the same parameters whose GPU work
+// overlaps (on different streams, or from threads that do not order their
+// streams) race on the array; issue them on one stream or order them.
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -39,10 +45,13 @@ struct StaticSlot {
   void* scratch = nullptr;  // device address of g_vfs_static_scratch on this device
   VfsPlan* plan = nullptr;
   VfsParams prm;
+  cudaEvent_t done = nullptr;  // recorded after each call's work on its stream
 };
 StaticSlot g_slots[kMaxDevices];
 std::mutex g_mutex;
 
+// Plain == on the doubles: vfs_plan_workspace_size (called first) rejects
+// non-finite parameters, so a NaN never reaches here and forces a rebuild.
 bool same_params(const VfsParams& a, const VfsParams& b) {
   return a.width == b.width && a.height == b.height && a.beta == b.beta && a.gamma == b.gamma &&
          a.alpha0 == b.alpha0 && a.alpha1 == b.alpha1 && a.timeStepLambda == b.timeStepLambda &&
@@ -78,7 +87,11 @@ int vfs_solve_stereo_static(const VfsParams* prm, const uint8_t* mask, size_t ma
     VFS_TRY_CUDA(cudaGetSymbolAddress(&p, g_vfs_static_scratch), "cudaGetSymbolAddress");
     slot.scratch = p;
   }
+  if (!slot.done) VFS_TRY_CUDA(cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming), "event create");
   if (slot.plan && !same_params(slot.prm, *prm)) {
+    // the previous call's kernels may still read this plan's textures and
+    // the schedule in the scratch: let them finish before both change
+    VFS_TRY_CUDA(cudaEventSynchronize(slot.done), "wait for the previous call");
     vfs_plan_destroy(slot.plan);
     slot.plan = nullptr;
   }
@@ -88,7 +101,9 @@ int vfs_solve_stereo_static(const VfsParams* prm, const uint8_t* mask, size_t ma
   }
   VFS_TRY(vfs_plan_set_mask(slot.plan, mask, mask_pitch, stream));
   VFS_TRY(vfs_plan_set_vector_fields(slot.plan, tvf_hw2, cvf_hw2, stream));
-  return vfs_plan_solve(slot.plan, img_ref, img_other, warp_out_hw2, stream);
+  VFS_TRY(vfs_plan_solve(slot.plan, img_ref, img_other, warp_out_hw2, stream));
+  VFS_TRY_CUDA(cudaEventRecord(slot.done, (cudaStream_t)stream), "event record");
+  return VFS_OK;
 }
 
 }  // extern "C"
