@@ -9,13 +9,22 @@ host-side orchestration (``Python/vfs.py``, ``Python/equidistant_cam.py``,
 the same call order, the same per-call texture objects (cudaArray copies) and a
 device-wide synchronisation after every launch, exactly as the reference does.
 
-Differences from running the reference under CuPy, all deliberate:
+Allocation has two modes.  The default (parity checking) differs from
+running the reference under CuPy, deliberately:
 
 * every array is allocated with zero-filled guard bands around it, so the
   reference kernels' out-of-bounds border reads (flat ``index-width`` at row 0,
   ``index+width`` at the last row) read zeros instead of whatever the CuPy
   memory pool had placed next to the array;
 * outputs that the reference allocates with ``cp.empty`` are zero-filled.
+
+``set_plain_allocation(True)`` (timing) allocates as CuPy does instead:
+``cp.empty`` becomes ``torch.empty`` (no fill kernel, no guard bands) and
+``cp.zeros`` becomes ``torch.zeros``, both from torch's caching allocator as
+CuPy's arrays come from its memory pool.  Every reference kernel writes each
+in-bounds element of its output, so the two modes give the same results
+wherever the mask keeps the border pixels out (the out-of-bounds reads need an
+unmasked pixel in the first or last row or column of some level).
 
 It is used by the GPU parity tests, the golden-fixture generator and the
 ``--impl reference`` arm of ``bench.py``; the product never imports it.
@@ -75,8 +84,26 @@ def _chk(rc: int, what: str) -> None:
 _DT_BYTES = {torch.uint8: 1, torch.int16: 2, torch.float32: 4, torch.int32: 4}
 
 
+_PLAIN = False
+
+
+def set_plain_allocation(enable: bool) -> None:
+    """Allocate as CuPy does (see the module docstring) instead of with
+    zero-filled guard bands."""
+    global _PLAIN
+    _PLAIN = bool(enable)
+
+
+def zeros(shape, dtype=torch.float32) -> torch.Tensor:
+    """``cp.zeros``: zero-filled (with zero guard bands unless plain)."""
+    return torch.zeros(shape, dtype=dtype, device="cuda") if _PLAIN else alloc(shape, dtype)
+
+
 def alloc(shape, dtype=torch.float32, guard_elems: int | None = None) -> torch.Tensor:
-    """Zero-filled CUDA tensor with zero guard bands before and after it."""
+    """``cp.empty``: a zero-filled CUDA tensor with zero guard bands before
+    and after it, or, with plain allocation, an uninitialised one."""
+    if _PLAIN:
+        return torch.empty(shape, dtype=dtype, device="cuda")
     n = int(np.prod(shape))
     if guard_elems is None:
         row = int(np.prod(shape[1:])) if len(shape) > 1 else n
@@ -412,9 +439,9 @@ class RefVFS:
             s2 = (*s, 2)
             s4 = (*s, 4)
             if s == self.sizes[-1]:
-                warpUV_ref = alloc(s2)
-                u = alloc(s)
-                u_ = alloc(s)
+                warpUV_ref = zeros(s2)
+                u = zeros(s)
+                u_ = zeros(s)
             ref_smoothed = self.gaussian(self.refs_to[k - 1], self.masks_to[k - 1], s)
             abc, eta = self.compute_tensor_eta(ref_smoothed, self.masks_to[k - 1])
             for _kw in range(self.param.nWarpIters):
@@ -422,9 +449,9 @@ class RefVFS:
                 other_warped = self.warping_image(self.others_to[k - 1], warpUV_ref)
                 derivatives = self.compute_derivatives(other_warped, self.refs_to[k - 1],
                                                        self.translations_to[k - 1])
-                p = alloc(s2)
-                q = alloc(s4)
-                v_ = alloc(s2)
+                p = zeros(s2)
+                q = zeros(s4)
+                v_ = zeros(s2)
                 tau = 1.
                 sigma = 1. / tau
                 u_before_solver = alloc(s)

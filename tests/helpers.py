@@ -1,6 +1,9 @@
 """Shared test inputs: parameter bags and synthetic pairs."""
 from __future__ import annotations
 
+import os
+import subprocess
+
 import numpy as np
 
 from vfs_b200.synthetic import make_pair
@@ -32,3 +35,14 @@ def pair(size, t=(0.1, 0.0, 0.0), seed=0, n_level=4, height=None):
 def bits(a) -> np.ndarray:
     a = np.ascontiguousarray(a)
     return a.view(np.uint32) if a.dtype == np.float32 else a
+
+
+def reference_dir() -> str:
+    """The reference checkout's Python directory (VFS_REFERENCE, else the
+    default oracle/refgpu/Makefile holds); "" when make cannot say."""
+    here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "refgpu")
+    try:
+        r = subprocess.run(["make", "-s", "-C", here, "print-ref"], capture_output=True, text=True, timeout=30)
+    except (OSError, subprocess.SubprocessError):
+        return ""
+    return r.stdout.strip() if r.returncode == 0 else ""

@@ -9,9 +9,9 @@ import os
 import numpy as np
 import pytest
 
-from helpers import pair
+from helpers import pair, reference_dir
 
-REF_COLORMAP = "/root/reference/Python/colormap.py"
+REF_COLORMAP = os.path.join(reference_dir() or os.devnull, "colormap.py")
 
 
 def _sample(tmp_path, R):

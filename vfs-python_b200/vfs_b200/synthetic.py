@@ -121,6 +121,43 @@ def rotation_xyz(rx: float, ry: float, rz: float) -> np.ndarray:
     return Rz @ Ry @ Rx
 
 
+def vector_fields(pair: StereoPair, t_scale=1.0):
+    """The pair's translation and calibration fields (tvf, cvf), (H, W, 2)
+    float32, from float64 camera math: what get_vector_fields(get_grid_zero,
+    cam, cam, R, t, t_scale) computes (Python/vector_field.py:28-56), so that
+    solvers fed from different implementations can be given identical
+    fields.  tvf = normalize((project(X + s0 t) - project(X - s1 t)) / 2) and
+    cvf = project(R X) - grid, X the unit ray of each pixel."""
+    s0, s1 = (t_scale, t_scale) if np.isscalar(t_scale) else t_scale
+    H, W = pair.img_ref.shape
+    f, cx, cy = pair.intrinsics
+    t = np.asarray(pair.t, np.float64).reshape(3)
+    yy, xx = np.meshgrid(np.arange(H, dtype=np.float64), np.arange(W, dtype=np.float64), indexing="ij")
+    grid = np.stack([xx, yy], -1)
+    X = _unproject(grid, f, cx, cy)
+    X = X / np.linalg.norm(X, axis=-1, keepdims=True)
+    d = (_project(X + s0 * t, f, cx, cy) - _project(X - s1 * t, f, cx, cy)) / 2
+    with np.errstate(invalid="ignore", divide="ignore"):
+        tvf = d / np.linalg.norm(d, axis=-1, keepdims=True)
+    cvf = _project(X @ np.asarray(pair.R, np.float64).T, f, cx, cy) - grid
+    return tvf.astype(np.float32), cvf.astype(np.float32)
+
+
+def uneven_workload(n_pairs: int = 32, seed: int = 0, sides=(480, 640, 800, 1024), t_range=(0.05, 0.2)):
+    """(side, t, seed) of each pair of the batched uneven workload: square
+    sides drawn uniformly from ``sides``, translation direction uniform on the
+    unit sphere with magnitude uniform in ``t_range`` metres, pair i seeded
+    with i."""
+    rng = np.random.default_rng(seed)
+    sz = rng.choice(list(sides), size=n_pairs)
+    out = []
+    for i in range(n_pairs):
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        out.append((int(sz[i]), tuple(d * rng.uniform(*t_range)), i))
+    return out
+
+
 def make_pair(size: int, t, seed: int = 0, n_level: int = 4, height: int | None = None, R=None) -> StereoPair:
     """One seeded pair at ``size`` x ``size`` (or ``height`` x ``size``);
     ``R`` (3x3) rotates the second view, X_other = R (X + t)."""
