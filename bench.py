@@ -8,15 +8,22 @@ rotation), 5-level pyramid at scale 0.5, 10 warps per level, 100 TGV
 iterations, lambda 50, alpha0 17, alpha1 1.2, beta 9, gamma 0.85, float32;
 solve_stereo followed by triangulate_flow.  The pair is synthetic (seeded
 range field + value-noise texture, see vfs_b200/synthetic.py): the reference
-publishes no benchmark data.
+publishes no benchmark data.  Both arms get the same images, mask and
+epipolar/calibration fields (float64 camera math, vfs_b200.synthetic.vector_fields).
 
 ``value``: device time of K steps with inputs resident in HBM (CUDA events on
 the solve's stream; L2 is flushed by writing 256 MiB between steps, outside
 the timed events).  ``e2e``: the same through the public Python API from
 pinned host images, with the host->device copy of both images and the
-device->host copy of the depth map inside the timed region.  With N > 1 GPUs
-each rank solves its own pair (weak scaling, no collective on the data path);
-times are the max over ranks.
+device->host copy of the depth map inside the timed region.  ``batched``: the
+32-pair uneven workload in one batched graph (pairs sharded over ranks by
+cost).  ``parity_vs_reference``: after the timed region, the same pair solved
+by the reference's own kernels (oracle/_ref), compared bit for bit.
+
+With N > 1 GPUs (``--gpus N`` starts the N ranks through torch.distributed.run
+when it is not already running under it) each rank solves its own pair (weak
+scaling, no collective on the data path); times are the max over ranks (NCCL).
+``--dry-run`` runs the rank plumbing on CPU with gloo and no GPU work.
 
 ``--impl reference``: the reference's own CUDA kernels (built from its sources
 into oracle/_ref) under the reference's host loop, which launches one kernel
@@ -142,30 +149,65 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_init():
+def launch_ranks(args) -> int:
+    """--gpus N outside torch.distributed.run: start N ranks through it (one
+    process per GPU, rendezvous on 127.0.0.1) with the same arguments; rank 0
+    prints the line.  Returns the launcher's exit status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
+def dist_init(dry_run=False):
     n = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    if not dry_run:
+        torch.cuda.set_device(local)
     if n > 1:
         import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                             device_id=torch.device("cuda", local))
+        if dry_run:
+            torch.distributed.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        else:
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                                 device_id=torch.device("cuda", local))
     return n, rank, local
 
 
 def max_over_ranks(x: float, n: int) -> float:
-    if n == 1:
-        return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item())
+    """Max over ranks (NCCL on GPUs, gloo in a dry run): time-like figures."""
+    from vfs_b200.distributed import max_over_ranks as _max
+    return float(x) if n == 1 else _max(x)
 
 
-def barrier(n):
+def barrier(n, dry_run=False):
     if n > 1:
         torch.distributed.barrier()
-    torch.cuda.synchronize()
+    if not dry_run:
+        torch.cuda.synchronize()
+
+
+def cpu_model() -> str:
+    """lscpu's model name of this host (or /proc/cpuinfo's)."""
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name:"):
+                return line.split(":", 1)[1].strip()
+    except (OSError, subprocess.SubprocessError):
+        pass
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def make_inputs(seed):
@@ -174,11 +216,13 @@ def make_inputs(seed):
 
 
 def setup_b200(pair, p):
+    """The drop-in VFS set up for one pair, with the pair's float64 fields
+    (the same arrays the reference arm and the parity check get)."""
     from vfs_b200 import VFS, EquidistantCam
-    from vfs_b200.vector_field import get_vector_fields, get_grid_zero
+    from vfs_b200.synthetic import vector_fields
     cam = EquidistantCam(pair.intrinsics)
     cam.setup_module()
-    tvf, cvf = get_vector_fields(get_grid_zero(pair.img_ref.shape), cam, cam, pair.R, pair.t, 1)
+    tvf, cvf = vector_fields(pair)
     vfs = VFS(p)
     vfs.setup_module()
     vfs.compute_pyramid_sizes()
@@ -236,10 +280,41 @@ def cpu_baseline_sample(pair, p, budget_s=20.0):
     per_px = lambda t: t / n0
     t_map = sum(n * (p.nWarpIters * (p.nSolverIters * per_px(t_iter) + per_px(t_warp)) + per_px(t_level))
                 for n in level_pixels(p))
-    return {"value": 1.0 / t_map, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"float64 NumPy oracle at 800x800: per-level + per-warp work once and {n_it} TGV iterations "
-                      f"({t_iter:.2f} s each), extrapolated by pixel-iterations to 5 levels x 10 warps x 100 "
-                      f"iterations ({t_map:.0f} s per map)"}
+    return {"value": 1.0 / t_map, "unit": UNIT, "cores": 1, "kind": "port", "cpu_model": cpu_model(),
+            "host_cpus": os.cpu_count(),
+            "sample": f"float64 NumPy oracle (one thread) at 800x800: the finest level's per-level and per-warp "
+                      f"work once and {n_it} TGV iterations ({t_iter:.2f} s each), extrapolated by pixel-iterations "
+                      f"to 5 levels x 10 warps x 100 iterations ({t_map:.0f} s per map)"}
+
+
+def parity_vs_reference(pair, p, flow, xyz):
+    """Checker, outside every timed region: the same pair (images, mask,
+    fields, parameters) solved by the reference's own kernels (oracle/_ref,
+    built from the reference's sources) under the reference's host loop,
+    compared with this run's flow and xyz.  Depth error over mask != 0 where
+    the reference depth is finite and in (0, 100] m."""
+    from oracle.refgpu import refpath
+    from vfs_b200.synthetic import vector_fields
+    tvf, cvf = vector_fields(pair)
+    r = refpath.RefVFS(p, "bench")
+    r.compute_pyramid_sizes()
+    r.create_mask_pyramid(pair.mask)
+    r.create_vector_field_pyramid(tvf, cvf)
+    cam = refpath.RefEquidistantCam(pair.intrinsics, "bench")
+    cam.setup_module()
+    rflow = r.solve_stereo(pair.img_ref, pair.img_other).cpu().numpy()
+    rxyz = r.triangulate_flow(cam, pair.t).cpu().numpy()
+    flow, xyz = np.ascontiguousarray(flow), np.ascontiguousarray(xyz)
+    zr, zo = rxyz[..., 2].astype(np.float64), xyz[..., 2].astype(np.float64)
+    sel = (pair.mask != 0) & np.isfinite(zr) & (zr > 0) & (zr <= 100)
+    both = np.isfinite(rflow) & np.isfinite(flow)
+    return {"checker": "reference kernels (oracle/_ref) on the same pair, fields and parameters",
+            "flow_values_differing": int(np.count_nonzero(rflow.view(np.uint32) != flow.view(np.uint32))),
+            "xyz_values_differing": int(np.count_nonzero(rxyz.view(np.uint32) != xyz.view(np.uint32))),
+            "flow_values": int(flow.size),
+            "max_abs_flow_diff_px": float(np.abs(rflow[both] - flow[both]).max()) if both.any() else None,
+            "median_rel_depth_err": float(np.median(np.abs(zo[sel] - zr[sel]) / zr[sel])) if sel.any() else None,
+            "depth_pixels_compared": int(sel.sum())}
 
 
 # ncu captures of the finest level's kernel, by TGV variant
@@ -267,6 +342,11 @@ def run_b200(args, n, rank, local):
         vfs.set_level_variants(level_choice)
     else:
         level_choice = vfs.autotune(ref_d, oth_d) if not args.no_autotune else None
+    tune_top = None
+    if level_choice and not args.level_variants:
+        from vfs_b200.autotune import last_table
+        tab = (last_table(vfs) or {}).get("table", {})
+        tune_top = [sorted(((round(ms[l], 3), int(v)) for v, ms in tab.items()))[:4] for l in range(N_LEVEL)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
@@ -313,6 +393,8 @@ def run_b200(args, n, rank, local):
         xyz = vfs.triangulate_flow(cam, pair.t)
         h_depth.copy_(xyz[:, :, 2], non_blocking=True)
 
+    xyz_np = step().cpu().numpy()  # one more solve, for the parity check
+    flow_np = vfs.warpUV.cpu().numpy()
     vfs.configure(timing=False)
     for _ in range(args.warmup):
         e2e_step()
@@ -346,6 +428,7 @@ def run_b200(args, n, rank, local):
                    "size": SIZE, "levels": N_LEVEL, "warps": N_WARP, "iterations": N_ITER, "lambda": 50.0,
                    "t": list(T), "tgv_kernel_default": args.iters_per_launch,
                    "tgv_kernel_per_level": level_choice, "cuda_graph": not args.no_graph,
+                   "autotune_fastest_per_level_ms_variant": tune_top,
                    "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "parallelism": f"dp{n} (independent pairs)"},
         "roofline": {"bound": "hbm", "kernel": f"k_tgv_reg (fused TGV iterations; finest level variant {fine})",
@@ -360,66 +443,65 @@ def run_b200(args, n, rank, local):
                 "d2h_bytes_per_step": 4 * SIZE * SIZE},
         "gpu_launches": int(kernels * args.steps),
         "clocks": clk.summary(),
-        "depth_check": {"median_rel_err_vs_ground_truth": float(np.median(
-            np.abs(depth[m] - pair.depth[m]) / pair.depth[m]))},
+        "depth_vs_ground_truth": {
+            "median_rel_err": float(np.median(np.abs(depth[m] - pair.depth[m]) / pair.depth[m])),
+            "note": "against the synthetic scene's true depth, not a parity figure: at Lambda 50 the "
+                    "reference's method itself drifts from the true depth"},
     }
     if not args.no_fwd_bwd:
-        # the same pair through the differentiable solve (no collective: every
-        # rank measures its own)
-        fb = fwd_bwd_timing(pair, p, plain_ms=1e3 * t_max / args.steps, flush=flush)
-        fb["ms_fwd_bwd"] = max_over_ranks(fb["ms_fwd_bwd"], n)
-        fb["ratio_to_forward"] = fb["ms_fwd_bwd"] / (1e3 * t_max / args.steps)
-        fb["fwd_bwd_per_s"] = n * 1e3 / fb["ms_fwd_bwd"]
-        line["fwd_bwd"] = fb
+        # the same pair through the differentiable solve (no collective on the
+        # data path: every rank measures its own), iterates checkpointed every
+        # 10 iterations and recomputed in the backward, and every state recorded
+        plain_ms = 1e3 * t_max / args.steps
+        fbs = {}
+        for ck in (10, 1):
+            fb = fwd_bwd_timing(pair, p, ckpt=ck, plain_ms=plain_ms, flush=flush)
+            fb["ms_fwd_bwd"] = max_over_ranks(fb["ms_fwd_bwd"], n)
+            fb["ratio_to_forward"] = fb["ms_fwd_bwd"] / plain_ms
+            fb["fwd_bwd_per_s"] = n * 1e3 / fb["ms_fwd_bwd"]
+            fbs[ck] = fb
+        line["fwd_bwd"] = fbs[10]
+        line["fwd_bwd_every_state_recorded"] = fbs[1]
+    del flush
+    if not args.no_batched:
+        line["batched"] = run_batched(args, n, rank, local, steps=max(3, min(args.steps, 10)))
+    if rank == 0 and not args.no_parity:
+        line["parity_vs_reference"] = parity_vs_reference(pair, p, flow_np, xyz_np)
     if n == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(pair, p, budget_s=args.cpu_budget)
     return line
 
 
 def _batched_pair(args):
-    """One pair of the batched workload (process-pool worker)."""
+    """One pair of the batched workload and its fields (process-pool worker)."""
     import os as _os
     import sys as _sys
     _sys.path[:0] = [ROOT, _os.path.join(ROOT, "vfs-python_b200")]
-    from vfs_b200.synthetic import make_pair
+    from vfs_b200.synthetic import make_pair, vector_fields
     size, t, seed = args
-    return make_pair(size, t, seed=seed, n_level=4)
+    pp = make_pair(size, t, seed=seed, n_level=4)
+    return pp, vector_fields(pp)
 
 
-def batched_workload(n_pairs=32, seed=0):
-    """Sizes drawn from {480, 640, 800, 1024}, translation direction uniform on
-    the sphere with magnitude in [0.05, 0.2] m, per-pair seeds."""
-    rng = np.random.default_rng(seed)
-    sizes = rng.choice([480, 640, 800, 1024], size=n_pairs)
-    out = []
-    for i in range(n_pairs):
-        d = rng.standard_normal(3)
-        d /= np.linalg.norm(d)
-        out.append((int(sizes[i]), tuple(d * rng.uniform(0.05, 0.2)), i))
-    return out
-
-
-def run_batched(args, n, rank, local):
+def run_batched(args, n, rank, local, steps=None):
     """32 pairs of uneven resolution, 4 levels x 10 warps x 50 iterations,
     solved as one batch (one graph, one TGV launch per pass over all pairs)."""
     import multiprocessing as mpc
     from vfs_b200.batch import VFSBatch
     from vfs_b200.distributed import shard, pair_cost
-    from vfs_b200 import EquidistantCam
-    from vfs_b200.vector_field import get_vector_fields, get_grid_zero
-    work = batched_workload()
+    from vfs_b200.synthetic import uneven_workload
+    steps = steps or args.steps
+    work = uneven_workload()
     costs = [pair_cost(s, s, 4, 2.0, 10, 50) for s, _, _ in work]
     mine = shard(costs, n, rank)
     with mpc.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
-        pairs = pool.map(_batched_pair, [work[i] for i in mine])
+        made = pool.map(_batched_pair, [work[i] for i in mine])
+    pairs = [m[0] for m in made]
     p = params()
     p.nLevel, p.nWarpIters, p.nSolverIters = 4, 10, 50
     sizes = [pp.img_ref.shape for pp in pairs]
     batch = VFSBatch(p, sizes)
-    for i, pp in enumerate(pairs):
-        cam = EquidistantCam(pp.intrinsics)
-        cam.setup_module()
-        tvf, cvf = get_vector_fields(get_grid_zero(pp.img_ref.shape), cam, cam, pp.R, pp.t, 1)
+    for i, (pp, (tvf, cvf)) in enumerate(made):
         batch.set_pair(i, pp.mask, tvf, cvf)
     refs = [torch.as_tensor(pp.img_ref).cuda() for pp in pairs]
     oths = [torch.as_tensor(pp.img_other).cuda() for pp in pairs]
@@ -433,7 +515,7 @@ def run_batched(args, n, rank, local):
     tot = 0.0
     tgv = 0.0
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
@@ -444,9 +526,11 @@ def run_batched(args, n, rank, local):
             tgv += batch.stats()["tgv_ms"] / 1e3
     barrier(n)
     t_max = max_over_ranks(tot, n)
-    value = len(work) * args.steps / t_max if n > 1 else len(pairs) * args.steps / t_max
-    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "strong",
+    value = len(work) * steps / t_max
+    del flush
+    batch.release()
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / steps, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (per-pair seeds)",
             "config": {"workload": "batched: 32 pairs, sides from {480, 640, 800, 1024}, random translation "
                                    "directions, 4 levels x 10 warps x 50 TGV iterations, one batched graph",
@@ -464,7 +548,7 @@ def run_batched800(args, n, rank, local):
     import multiprocessing as mpc
     from vfs_b200.batch import VFSBatch
     from vfs_b200 import EquidistantCam
-    from vfs_b200.vector_field import get_vector_fields, get_grid_zero
+    from vfs_b200.synthetic import vector_fields
     seeds = [rank * args.pairs + i for i in range(args.pairs)]
     with mpc.get_context("spawn").Pool(min(args.pairs, os.cpu_count() or 1)) as pool:
         pairs = pool.map(make_inputs, seeds)
@@ -474,8 +558,7 @@ def run_batched800(args, n, rank, local):
     for i, pp in enumerate(pairs):
         cam = EquidistantCam(pp.intrinsics)
         cam.setup_module()
-        tvf, cvf = get_vector_fields(get_grid_zero(pp.img_ref.shape), cam, cam, pp.R, pp.t, 1)
-        batch.set_pair(i, pp.mask, tvf, cvf)
+        batch.set_pair(i, pp.mask, *vector_fields(pp))
         cams.append(cam)
     refs = [torch.as_tensor(pp.img_ref).cuda() for pp in pairs]
     oths = [torch.as_tensor(pp.img_other).cuda() for pp in pairs]
@@ -516,13 +599,16 @@ def run_batched800(args, n, rank, local):
 
 
 def run_reference(args, n, rank, local):
+    """The reference's CUDA kernels (oracle/_ref) under the reference's host
+    loop (Python/vfs.py:460-559), allocating as CuPy does (no fill kernels for
+    cp.empty arrays), on the same pair, fields and parameters as the B200 arm;
+    L2 flushed between steps outside the timed events, as in the B200 arm."""
     from oracle.refgpu import refpath
+    from vfs_b200.synthetic import vector_fields
+    refpath.set_plain_allocation(True)
     p = params()
     pair = make_inputs(seed=0)
-    from oracle.np64 import vfs64 as V
-    cam64 = V.EquidistantCam64(pair.intrinsics)
-    tvf, cvf = V.get_vector_fields(V.get_grid_zero(pair.img_ref.shape), cam64, cam64, pair.R, pair.t, 1)
-    tvf, cvf = tvf.astype(np.float32), cvf.astype(np.float32)
+    tvf, cvf = vector_fields(pair)
     r = refpath.RefVFS(p, "bench")
     r.compute_pyramid_sizes()
     r.create_mask_pyramid(pair.mask)
@@ -536,30 +622,37 @@ def run_reference(args, n, rank, local):
 
     for _ in range(args.warmup):
         step()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        step()
-    e1.record()
-    torch.cuda.synchronize()
-    el = e0.elapsed_time(e1) / 1e3
+    el = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step()
+            e1.record()
+            e1.synchronize()
+            el += e0.elapsed_time(e1) / 1e3
     value = args.steps / el
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "impl": "reference", "data": "synthetic (same pair as the b200 arm, seed 0)",
+        "dtype": "f32", "impl": "reference", "data": "synthetic (same pair and fields as the b200 arm, seed 0)",
         "config": {"workload": "800x800 equidistant fisheye pair, 5 levels x 10 warps x 100 TGV iterations, "
                                "solve_stereo + triangulate_flow",
                    "size": SIZE, "levels": N_LEVEL, "warps": N_WARP, "iterations": N_ITER, "lambda": 50.0,
                    "t": list(T), "parallelism": "single GPU",
-                   "l2": "not flushed (the reference's host loop synchronises after every launch)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "allocation": "as CuPy: cp.empty -> uninitialised, cp.zeros -> zero-filled (torch's caching "
+                                 "allocator in place of CuPy's pool)",
+                   "l2": "flushed between steps (256 MiB write outside the timed events)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "cpu_model": cpu_model(),
                          "sample": f"{args.steps} full 800x800 solves: the reference's CUDA kernels on the B200, "
                                    "launched and synchronised one at a time by one host thread"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
         "wall_s": time.perf_counter() - t0,
     }
 
@@ -795,6 +888,29 @@ def run_grad(args, n, rank, local):
     }
 
 
+def dry_run(args, n, rank):
+    """The multi-rank plumbing without GPU work (gloo on CPU): each rank takes
+    its cost-balanced shard of the batched workload's pairs, the max of a
+    per-rank time, and the sum over ranks of a per-rank theta gradient, through
+    the same helpers the GPU runs use."""
+    from vfs_b200.distributed import shard, pair_cost
+    from vfs_b200.synthetic import uneven_workload
+    work = uneven_workload()
+    costs = [pair_cost(s, s, 4, 2.0, 10, 50) for s, _, _ in work]
+    mine = shard(costs, n, rank)
+    t_max = max_over_ranks(1.0 + rank, n)
+    g = torch.tensor([rank + 1.0, 2.0 * rank, 0.5, -rank, 3.0], dtype=torch.float64)
+    if n > 1:
+        torch.distributed.all_reduce(g)
+        shards = [None] * n
+        torch.distributed.all_gather_object(shards, mine)
+    else:
+        shards = [mine]
+    return {"dry_run": True, "n_gpus": n, "world_size": n, "workload": "batched uneven (32 pairs)",
+            "shards": shards, "shard_costs": [sum(costs[i] for i in sh) for sh in shards],
+            "max_over_ranks": t_max, "theta_grad_sum": g.tolist()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -827,6 +943,12 @@ def main():
     ap.add_argument("--trace-variant", type=int, default=0,
                     help="with --profile-grad: TGV variant of the recording forward, one with a recording "
                          "form (0: the default, 134)")
+    ap.add_argument("--no-batched", action="store_true", help="single: skip the batched uneven workload")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="single: skip the parity check against the reference kernels")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="rank plumbing only, on CPU with gloo: shards, max-over-ranks and the theta-gradient "
+                         "sum; no GPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--profile-case", action="store_true",
@@ -838,6 +960,17 @@ def main():
         args.steps = 10 if args.impl == "reference" else {"single": 40, "batched": 10, "batched800": 10, "grad": 10,
                                                             "learn": 3}[args.workload]
     args.warmup = max(args.warmup, 1)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args))
+    if args.dry_run:
+        n, rank, local = dist_init(dry_run=True)
+        line = dry_run(args, n, rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if n > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
     if args.profile_case and args.profile_grad:
         torch.cuda.set_device(0)
         from vfs_b200 import DepthSolver, EquidistantCam

@@ -59,3 +59,28 @@ def test_two_gloo_ranks():
     assert sorted(m0 + m1) == list(range(32)) and not set(m0) & set(m1)
     assert t0 == t1 == 2.5
     assert g0 == g1 == {"Lambda": 3.0, "alpha0": 2.0}
+
+
+def test_bench_launches_two_ranks_dry_run():
+    """`bench.py --gpus 2` starts two ranks through torch.distributed.run; in a
+    dry run (gloo, no GPU) rank 0 prints one line with n_gpus 2, disjoint
+    cost-balanced shards covering the batch, and the summed theta gradient."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ)
+    env.pop("WORLD_SIZE", None)
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--dry-run"],
+                       capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    line = lines[0]
+    assert line["n_gpus"] == 2 and line["dry_run"]
+    a, b = line["shards"]
+    assert sorted(a + b) == list(range(32)) and not set(a) & set(b)
+    c0, c1 = line["shard_costs"]
+    assert max(c0, c1) / min(c0, c1) < 1.05
+    assert line["max_over_ranks"] == 2.0
+    assert line["theta_grad_sum"] == [3.0, 2.0, 1.0, -1.0, 6.0]
