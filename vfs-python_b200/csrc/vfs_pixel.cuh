@@ -33,6 +33,21 @@ struct SolverConsts {
   const float2* dscale;
 };
 
+// ---------------------------------------------------------------- division helpers
+// of the two-pixel TGV kernels (vfs_tgv_pair.cuh), which divide by a per-pixel
+// constant y through its reciprocal.  2^-60 <= |v| <= 2^60 (false for zeros,
+// subnormals, Inf and NaN): the range where the reciprocal method is exact.
+__device__ __forceinline__ bool div_range(float v) {
+  return (__float_as_uint(v) & 0x7fffffffu) - 0x21800000u <= 0x3C000000u;
+}
+// The eta a step divides by: below the reference's eps (1e-7) the reference
+// uses tau itself instead of tau / eta, and tau / 1 == tau.
+__device__ __forceinline__ float eta_used(float e) { return fabsf(e) < 1E-7f ? 1.f : e; }
+// RN(1 / y) in the range above, NaN outside it (the kernels then divide with '/').
+__device__ __forceinline__ float recip_or_nan(float y) {
+  return div_range(y) ? __frcp_rn(y) : __int_as_float(0x7fffffff);
+}
+
 // ---------------------------------------------------------------- K7 tensor
 // computeEta, Python/vfs.cu:228-237.
 __device__ __forceinline__ float3 compute_eta(float a, float b, float c, float a11, float a004) {

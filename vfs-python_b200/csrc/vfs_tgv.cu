@@ -197,6 +197,7 @@ cudaError_t launch_block(const TgvState& in, const TgvState& out, const TgvConst
 }  // namespace vfs
 
 #include "vfs_tgv_reg.cuh"
+#include "vfs_tgv_pair.cuh"
 
 namespace vfs {
 namespace {
@@ -214,6 +215,23 @@ cudaError_t prepare_reg() {
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_tgv_reg_batch<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)RegGeom<K, TX, TY>::smem_bytes());
+}
+
+template <int K, int TX, int TY, int NT>
+cudaError_t prepare_pair() {
+  cudaError_t e = cudaFuncSetAttribute(k_tgv_pair<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)pair_smem_bytes<K, TX, TY>(NT));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tgv_pair_batch<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)pair_smem_bytes<K, TX, TY>(NT));
+}
+
+template <int K, int TX, int TY, int NT>
+cudaError_t batch_pair(const TgvBatchItem* items, int n_items, int total_tiles, int parity, const float3* sched,
+                       int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
+  k_tgv_pair_batch<K, TX, TY, NT><<<total_tiles, NT, pair_smem_bytes<K, TX, TY>(NT), s>>>(items, n_items, parity,
+                                                                                          sched, it0, niter, kc);
+  return cudaGetLastError();
 }
 
 template <int K, int TX, int TY, int NT>
@@ -264,8 +282,17 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   return e;
 }
 
+template <int K, int TX, int TY, int NT>
+cudaError_t launch_pair(const TgvState& in, const TgvState& out, const TgvConsts& c, const float3* sched, int it0,
+                        int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
+  dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);
+  PdlLaunch L(grid, NT, pair_smem_bytes<K, TX, TY>(NT), s);
+  return cudaLaunchKernelEx(&L.cfg, k_tgv_pair<K, TX, TY, NT>, in, out, c, sched, it0, niter, kc, h, w);
+}
+
 // Compiled variants: id -> (implementation, iterations per launch, tile).
 // Ids below 100 keep all state in shared memory; ids 1xx are register-owned.
+// Ids 3xx are the two-pixel lockstep kernels (vfs_tgv_pair.cuh).
 // Ids 22x have tiles sized so that a pyramid level of side S = 12 T covers
 // at most 144 tiles, one per SM of the 148: the 1024-thread kernels hold one
 // CTA per SM, so 169 tiles of a power-of-two side would need a second wave
@@ -320,7 +347,13 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   X(223, reg, 5, 17, 17, 1024)       \
   X(224, reg, 6, 9, 9, 736)          \
   X(225, reg, 4, 11, 11, 544)        \
-  X(226, reg, 4, 27, 27, 1024)
+  X(226, reg, 4, 27, 27, 1024)       \
+  X(320, pair, 3, 34, 34, 1024)      \
+  X(321, pair, 3, 36, 36, 1024)      \
+  X(334, pair, 4, 32, 32, 1024)      \
+  X(326, pair, 3, 22, 22, 512)       \
+  X(322, pair, 4, 17, 17, 448)       \
+  X(324, pair, 6, 8, 8, 352)
 
 // Register-owned variants also compiled in recording form (every
 // iteration's state written out), for the reverse mode's recomputation.
@@ -407,7 +440,7 @@ bool tgv_tile_shape(int variant, int* tx, int* ty) {
   case id:                                \
     *tx = TX;                             \
     *ty = TY;                             \
-    return std::string(#impl) == "reg";
+    return std::string(#impl) != "block";
     VFS_TGV_VARIANTS(VFS_SHAPE)
 #undef VFS_SHAPE
     default: return false;

@@ -1,0 +1,500 @@
+// Two-pixel lockstep variant of the temporally blocked TGV kernel (included
+// by vfs_tgv.cu; same geometry, same flat addressing, same per-pixel results).
+//
+// Thread t owns window pixels e0 = t and e1 = t + NT and carries them through
+// every step together, as the two lanes of float2 values: on sm_100 one
+// FFMA2/FADD2/FMUL2 instruction performs the fused multiply-add / add /
+// multiply of both lanes, each rounded exactly as the scalar instruction, so
+// the arithmetic of the solver step costs half the instructions of a
+// pixel-per-lane formulation while producing the same bits.
+//
+// Shared memory holds "pair records": the value of a quantity for both
+// pixels of a thread side by side, so one 8- or 16-byte access loads both
+// lanes of one or two quantities straight into a register pair.  The flat
+// neighbour of a thread's pixels (e +- 1, e +- WX) is the same lane of the
+// record of thread t +- 1 or t +- WX, except across the seam between the two
+// halves of the window (t + 1 == NT, t + WX >= NT, t == 0, t < WX), where the
+// neighbour is the other lane of the record at t +- 1 -+ NT; those loads take
+// the other lane (a register move in the few threads concerned).
+//
+// Which pixels a step computes: the tile's cone of dependence shrinks by
+// (2, 1) pixels per iteration (vfs_tgv.cu).  A thread computes both of its
+// pixels whenever either is inside the current region; a pixel outside the
+// region gets a value that nothing inside any later region reads, so it may
+// be anything.  Pixels whose mask code is not "unmasked with all four
+// neighbours unmasked" (masked pixels, the pixels along the mask border,
+// pixels outside the image) take the scalar per-pixel functions of
+// vfs_pixel.cuh lane by lane; the packed path handles the interior.
+//
+// Division.  tau / eta (eta a per-level constant of each pixel) and rho / dIu
+// use r = RN(1 / y), formed once per level (eta) or per warp (dIu), and two
+// corrections (Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): q0 = RN(x r) is
+// within 1.5 ulp of x / y, q1 = RN(q0 + (x - y q0) r) within an ulp, and
+// q2 = RN(q1 + (x - y q1) r) is the correctly rounded quotient RN(x / y),
+// the IEEE division's result, provided x, y, the quotient and the remainders
+// are normal numbers.  The kernel uses it only where 2^-60 <= |x|, |y| <= 2^60
+// (tau from the host's schedule is checked per iteration, rho per pixel, and
+// the reciprocal of an eta or dIu outside the range is stored as NaN); any
+// lane whose fast quotient is NaN is divided with '/' instead, which also
+// covers NaN inputs.
+#pragma once
+
+namespace vfs {
+namespace {
+
+__device__ __forceinline__ float2 f2(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b: one rounding of a + (-1 * b), the product being exact
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.f), a); }
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+
+// RN(x / y) of both lanes from ny = -y and r = RN(1 / y) (see the file
+// comment); a lane whose result is NaN is divided with '/'.
+__device__ __forceinline__ float2 pdiv(float2 x, float2 ny, float2 r) {
+  const float2 q0 = pmul(x, r);
+  const float2 e0 = pfma(q0, ny, x);
+  const float2 q1 = pfma(e0, r, q0);
+  const float2 e1 = pfma(q1, ny, x);
+  float2 q = pfma(e1, r, q1);
+  if (q.x != q.x) q.x = x.x / -ny.x;
+  if (q.y != q.y) q.y = x.y / -ny.y;
+  return q;
+}
+
+// How the reference's threshold step rounds its multiply-adds (the compiler
+// fuses some of them into FMAs): uTauGtp = u_ + tauEtaU (gx + gy), rho =
+// dIu (uTauGtp - u) + dIz, and uTauGtp - u +- lambda tauEtaU dIu.
+constexpr bool kFuseUT = true, kFuseRho = true, kFuseLo = true, kFuseHi = true;
+
+template <int K, int TX, int TY>
+struct PairGeom {
+  static constexpr int WX = TX + 3 * K;
+  static constexpr int WY = TY + 3 * K;
+  static constexpr int N = WX * WY;
+};
+
+// Shared-memory pair records of NT threads.
+template <int NT>
+struct PairSmem {
+  float4* base;
+  // (u_0, u_1, vx0, vx1), (vy0, vy1, -, -): the bar variables
+  __device__ __forceinline__ float4& uvA(int t) const { return base[t]; }
+  __device__ __forceinline__ float2& uvB(int t) const { return reinterpret_cast<float2*>(base + NT)[2 * t]; }
+  // (qx0, qx1, qy0, qy1), (qz0, qz1, qw0, qw1)
+  __device__ __forceinline__ float4& qA(int t) const { return base[2 * NT + t]; }
+  __device__ __forceinline__ float4& qB(int t) const { return base[3 * NT + t]; }
+  // (tpx0, tpx1, tpy0, tpy1)
+  __device__ __forceinline__ float4& tp(int t) const { return base[4 * NT + t]; }
+  // (-eta'.x0, -eta'.x1, rx0, rx1), the same for eta.y, eta.z, and
+  // (-dIu0, -dIu1, riu0, riu1)
+  __device__ __forceinline__ float4& cE(int t) const { return base[5 * NT + t]; }
+  __device__ __forceinline__ float4& cY(int t) const { return base[6 * NT + t]; }
+  __device__ __forceinline__ float4& cZ(int t) const { return base[7 * NT + t]; }
+  __device__ __forceinline__ float4& cU(int t) const { return base[8 * NT + t]; }
+  static constexpr int kRecords = 9;
+  // scalar view of window pixel e: component c of a record family whose
+  // records hold two components (c = 0, 1) per lane
+  __device__ __forceinline__ float& at(int family, int e, int c) const {
+    const int lane = e >= NT;
+    const int t = e - lane * NT;
+    return reinterpret_cast<float*>(base + family * NT + t)[2 * c + lane];
+  }
+};
+
+enum PairFamily { fUVA = 0, fUVB = 1, fQA = 2, fQB = 3, fTP = 4, fCE = 5, fCY = 6, fCZ = 7 };
+
+template <int K, int TX, int TY>
+constexpr size_t pair_smem_bytes(int nt) {
+  return (size_t)PairSmem<1>::kRecords * nt * 16 + 5 * K * sizeof(float);
+}
+
+// The last phase (1-based: the dual step of iteration s is phase 2s-1, its
+// threshold and primal steps phase 2s) whose region contains window pixel
+// (wx, wy) when the launch runs k iterations; 0 if none.  The regions are
+// nested, so a pixel takes part in phases 1 .. last.
+template <int K, int TX, int TY>
+__device__ __forceinline__ int last_phase(int wx, int wy, int k) {
+  int last = 0;
+  for (int s = 1; s <= k; ++s) {
+    const int lo_d = 2 * K - 2 * (k - s) - 1, lo_p = lo_d + 1;
+    const int hiX = 2 * K + TX + (k - s), hiY = 2 * K + TY + (k - s);
+    if (wx >= lo_d && wx < hiX && wy >= lo_d && wy < hiY) last = 2 * s - 1;
+    if (wx >= lo_p && wx < hiX && wy >= lo_p && wy < hiY) last = 2 * s;
+  }
+  return last;
+}
+
+template <int K, int TX, int TY, int NT>
+__device__ __forceinline__ void tgv_pair_tile(const TgvState& in, const TgvState& out, const TgvConsts& cst,
+                                              const float3* __restrict__ sched, int it0, int niter,
+                                              const SolverConsts& kc, int h, int w, int x0, int y0) {
+  using G = PairGeom<K, TX, TY>;
+  constexpr int WX = G::WX, N = G::N;
+  static_assert(N <= 2 * NT && WX < NT, "window must fit two pixels per thread");
+  static_assert(2 * K < 64, "the last phase must fit 6 bits");
+  extern __shared__ float4 smem_raw[];
+  const PairSmem<NT> S{smem_raw};
+  float* const sSch = reinterpret_cast<float*>(smem_raw + PairSmem<NT>::kRecords * NT);
+
+  const int t = threadIdx.x;
+  const long n = (long)h * w;
+  const long base = (long)(y0 - 2 * K) * w + (x0 - 2 * K);
+  const int e0 = t, e1 = t + NT;
+
+  // When launched as a programmatic dependent of the previous TGV launch this
+  // CTA may start before that launch ends: the per-warp constants are read
+  // first, the state (which that launch writes) only after griddepcontrol.wait.
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  const int k = niter < K ? niter : K;
+  if (t < 5 * k) {  // this launch's step sizes and dual-step scales
+    const int i = t / 5, c = t - 5 * i;
+    sSch[t] = c < 3 ? reinterpret_cast<const float*>(sched + it0 + i)[c]
+                    : reinterpret_cast<const float*>(kc.dscale + it0 + i)[c - 3];
+  }
+
+  // ---- per-warp constants of both pixels
+  float2 ra, rb, rc, iu, iz;
+  int code[2], last[2];
+  {
+    float4 rcp[2];
+    float ex[2], ey[2], ez[2];
+    const float nan = __int_as_float(0x7fffffff);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int e = j ? e1 : e0;
+      const int wy = e / WX, wx = e - wy * WX;
+      const long f = base + (long)wy * w + wx;
+      const bool ok = e < N && f >= 0 && f < n;
+      const float a = ok ? cst.a[f] : 0.f, b = ok ? cst.b[f] : 0.f, c = ok ? cst.c[f] : 0.f;
+      const float du = ok ? cst.iu[f] : 0.f, dz = ok ? cst.iz[f] : 0.f;
+      if (j) ra.y = a, rb.y = b, rc.y = c, iu.y = du, iz.y = dz;
+      else ra.x = a, rb.x = b, rc.x = c, iu.x = du, iz.x = dz;
+      ex[j] = ok ? cst.ex[f] : 1.f;
+      ey[j] = ok ? cst.ey[f] : 1.f;
+      ez[j] = ok ? cst.ez[f] : 1.f;
+      // without reciprocal records every division takes '/' (NaN reciprocals)
+      rcp[j] = ok && cst.rcp ? cst.rcp[f] : make_float4(nan, nan, nan, nan);
+      code[j] = ok ? cst.code[f] : 0;
+      last[j] = e < N ? last_phase<K, TX, TY>(wx, wy, k) : 0;
+    }
+    S.cE(t) = make_float4(-eta_used(ex[0]), -eta_used(ex[1]), rcp[0].x, rcp[1].x);
+    S.cY(t) = make_float4(-eta_used(ey[0]), -eta_used(ey[1]), rcp[0].y, rcp[1].y);
+    S.cZ(t) = make_float4(-eta_used(ez[0]), -eta_used(ez[1]), rcp[0].z, rcp[1].z);
+    S.cU(t) = make_float4(-iu.x, -iu.y, rcp[0].w, rcp[1].w);
+  }
+  // class 0: both pixels unmasked with all four neighbours unmasked (packed
+  // path); 1: both masked (zero state); 2: lane by lane.  info bits 0-4 /
+  // 8-12: the mask codes, 16-21 / 24-29: the last phases, 30-31: the class.
+  const unsigned cls =
+      (code[0] == 0x1F && code[1] == 0x1F) ? 0u : (!(code[0] & kSelf) && !(code[1] & kSelf)) ? 1u : 2u;
+  const unsigned info = (unsigned)code[0] | (unsigned)code[1] << 8 | (unsigned)last[0] << 16 |
+                        (unsigned)last[1] << 24 | cls << 30;
+
+  // a tile whose pixels are all masked ends with zero state (masked pixels
+  // are written 0 every iteration): write that and skip the iterations
+  int live = 0;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int e = j ? e1 : e0;
+    const int wy = e / WX, wx = e - wy * WX;
+    const int tx = wx - 2 * K, ty = wy - 2 * K;
+    if (e < N && tx >= 0 && tx < TX && ty >= 0 && ty < TY && x0 + tx < w && y0 + ty < h && (code[j] & kSelf))
+      live = 1;
+  }
+  live = __syncthreads_or(live);
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  if (!live) {
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int e = j ? e1 : e0;
+      const int wy = e / WX, wx = e - wy * WX;
+      const int tx = wx - 2 * K, ty = wy - 2 * K;
+      if (e >= N || tx < 0 || tx >= TX || ty < 0 || ty >= TY) continue;
+      const int X = x0 + tx, Y = y0 + ty;
+      if (X >= w || Y >= h) continue;
+      const long f = (long)Y * w + X;
+      out.u[f] = out.ub[f] = out.vbx[f] = out.vby[f] = out.px[f] = out.py[f] = 0.f;
+      out.qx[f] = out.qy[f] = out.qz[f] = out.qw[f] = 0.f;
+    }
+    return;
+  }
+
+  // ---- state of both pixels
+  float2 u, px, py;
+  {
+    float v[2][10];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int e = j ? e1 : e0;
+      const int wy = e / WX, wx = e - wy * WX;
+      const long f = base + (long)wy * w + wx;
+      const bool ok = e < N && f >= 0 && f < n;
+      v[j][0] = ok ? in.u[f] : 0.f;
+      v[j][1] = ok ? in.ub[f] : 0.f;
+      v[j][2] = ok ? in.vbx[f] : 0.f;
+      v[j][3] = ok ? in.vby[f] : 0.f;
+      v[j][4] = ok ? in.px[f] : 0.f;
+      v[j][5] = ok ? in.py[f] : 0.f;
+      v[j][6] = ok ? in.qx[f] : 0.f;
+      v[j][7] = ok ? in.qy[f] : 0.f;
+      v[j][8] = ok ? in.qz[f] : 0.f;
+      v[j][9] = ok ? in.qw[f] : 0.f;
+    }
+    u = make_float2(v[0][0], v[1][0]);
+    px = make_float2(v[0][4], v[1][4]);
+    py = make_float2(v[0][5], v[1][5]);
+    S.uvA(t) = make_float4(v[0][1], v[1][1], v[0][2], v[1][2]);
+    S.uvB(t) = make_float2(v[0][3], v[1][3]);
+    S.qA(t) = make_float4(v[0][6], v[1][6], v[0][7], v[1][7]);
+    S.qB(t) = make_float4(v[0][8], v[1][8], v[0][9], v[1][9]);
+  }
+  __syncthreads();
+
+  for (int s = 1; s <= k; ++s) {
+    const float* const sc = sSch + 5 * (s - 1);
+    const float tau = sc[1], mu = sc[2];
+    const float scaleP = sc[3], scaleQ = sc[4];  // alpha1 sigma / etaP, alpha0 sigma / etaQ
+    const unsigned cl = info >> 30;
+    const int lastP = max((int)(info >> 16 & 63u), (int)(info >> 24 & 63u));
+    // ---------------------------------------------------------------- dual step
+    if (2 * s - 1 <= lastP) {
+      if (cl == 0) {
+        // neighbour records E and S, across the seam the other lane
+        const bool seamE = t + 1 == NT, seamS = t + WX >= NT;
+        const int tE = seamE ? 0 : t + 1, tS = seamS ? t + WX - NT : t + WX;
+        const float4 cA = S.uvA(t);
+        const float2 cB = S.uvB(t);
+        float4 eA = S.uvA(tE);
+        float2 eB = S.uvB(tE);
+        float4 sA = S.uvA(tS);
+        float2 sB = S.uvB(tS);
+        if (seamE) eA.x = eA.y, eA.z = eA.w, eB.x = eB.y;
+        if (seamS) sA.x = sA.y, sA.z = sA.w, sB.x = sB.y;
+        const float2 uc = lo2(cA), vcx = hi2(cA), vcy = cB;
+        // updateDualVariables with E and S unmasked (Python/vfs.cu:352-408)
+        const float2 gUx = psub(psub(lo2(eA), uc), vcx);
+        const float2 gVx = psub(hi2(eA), vcx), gVw = psub(eB, vcy);
+        const float2 gUy = psub(psub(lo2(sA), uc), vcy);
+        const float2 gVy = psub(sB, vcy), gVz = psub(hi2(sA), vcx);
+        const float2 tux = pfma(ra, gUx, pmul(rc, gUy)), tuy = pfma(rc, gUx, pmul(rb, gUy));
+        float2 upx = pfma(f2(scaleP), tux, px), upy = pfma(f2(scaleP), tuy, py);
+        // projection onto the unit ball: a lane with |up|^2 < 0.98 has a norm
+        // below 1, so max(hypot, 1) is 1 and up / 1 == up; others as the reference
+        const float2 n2 = pfma(upx, upx, pmul(upy, upy));
+        if (!(n2.x < 0.98f)) {
+          const float nr = fmaxf(hypotf(upx.x, upy.x), 1.0f);
+          upx.x = upx.x / nr, upy.x = upy.x / nr;
+        }
+        if (!(n2.y < 0.98f)) {
+          const float nr = fmaxf(hypotf(upx.y, upy.y), 1.0f);
+          upx.y = upx.y / nr, upy.y = upy.y / nr;
+        }
+        px = upx, py = upy;
+        const float2 tpx = pfma(ra, upx, pmul(rc, upy)), tpy = pfma(rc, upx, pmul(rb, upy));
+        S.tp(t) = make_float4(tpx.x, tpx.y, tpy.x, tpy.y);
+        const float4 qa = S.qA(t), qb = S.qB(t);
+        float2 qx = pfma(f2(scaleQ), gVx, lo2(qa)), qy = pfma(f2(scaleQ), gVy, hi2(qa));
+        float2 qz = pfma(f2(scaleQ), gVz, lo2(qb)), qw = pfma(f2(scaleQ), gVw, hi2(qb));
+        const float2 m2 = pfma(qx, qx, pfma(qy, qy, pfma(qz, qz, pmul(qw, qw))));
+        if (!(m2.x < 0.98f)) {
+          const float nr = fmaxf(norm4df(qx.x, qy.x, qz.x, qw.x), 1.0f);
+          qx.x = qx.x / nr, qy.x = qy.x / nr, qz.x = qz.x / nr, qw.x = qw.x / nr;
+        }
+        if (!(m2.y < 0.98f)) {
+          const float nr = fmaxf(norm4df(qx.y, qy.y, qz.y, qw.y), 1.0f);
+          qx.y = qx.y / nr, qy.y = qy.y / nr, qz.y = qz.y / nr, qw.y = qw.y / nr;
+        }
+        S.qA(t) = make_float4(qx.x, qx.y, qy.x, qy.y);
+        S.qB(t) = make_float4(qz.x, qz.y, qw.x, qw.y);
+      } else if (cl == 1) {
+        px = py = f2(0.f);
+        S.tp(t) = make_float4(0.f, 0.f, 0.f, 0.f);
+        S.qA(t) = S.qB(t) = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {
+#pragma unroll 1
+        for (int j = 0; j < 2; ++j) {
+          if (2 * s - 1 > (int)(info >> (16 + 8 * j) & 63u)) continue;
+          const int e = j ? e1 : e0;
+          const uint8_t cd = (uint8_t)(info >> (8 * j) & 31u);
+          float2 p = j ? make_float2(px.y, py.y) : make_float2(px.x, py.x), tp = make_float2(0.f, 0.f);
+          float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (cd & kSelf) {
+            q = make_float4(S.at(fQA, e, 0), S.at(fQA, e, 1), S.at(fQB, e, 0), S.at(fQB, e, 1));
+            auto uv = [&](int i) { return make_float3(S.at(fUVA, i, 0), S.at(fUVA, i, 1), S.at(fUVB, i, 0)); };
+            const float3 c = uv(e), cE = uv(e + 1), cW = uv(e - 1), cS = uv(e + WX), cN = uv(e - WX);
+            dual_px(cd, c.x, make_float2(c.y, c.z), cE.x, make_float2(cE.y, cE.z), cW.x, make_float2(cW.y, cW.z),
+                    cS.x, make_float2(cS.y, cS.z), cN.x, make_float2(cN.y, cN.z),
+                    make_float3(j ? ra.y : ra.x, j ? rb.y : rb.x, j ? rc.y : rc.x), scaleP, scaleQ, &p, &tp, &q);
+          } else {
+            p = make_float2(0.f, 0.f);
+          }
+          if (j) px.y = p.x, py.y = p.y;
+          else px.x = p.x, py.x = p.y;
+          S.at(fTP, e, 0) = tp.x;
+          S.at(fTP, e, 1) = tp.y;
+          S.at(fQA, e, 0) = q.x;
+          S.at(fQA, e, 1) = q.y;
+          S.at(fQB, e, 0) = q.z;
+          S.at(fQB, e, 1) = q.w;
+        }
+      }
+    }
+    __syncthreads();
+    // ------------------------------------------------- threshold + primal steps
+    if (2 * s <= lastP) {
+      if (cl == 0) {
+        const bool seamW = t == 0, seamN = t < WX;
+        const int tW = seamW ? NT - 1 : t - 1, tN = seamN ? t + NT - WX : t - WX;
+        const bool fast_tau = div_range(tau);
+        const float2 tau2 = f2(tau);
+        // l1Thresholding with all four neighbours unmasked (Python/vfs.cu:444-494)
+        const float4 tc = S.tp(t);
+        float4 tw = S.tp(tW), tn = S.tp(tN);
+        if (seamW) tw.y = tw.x;
+        if (seamN) tn.w = tn.z;
+        const float2 gTx = psub(lo2(tc), lo2(tw)), gTy = psub(hi2(tc), hi2(tn));
+        const float4 ce = S.cE(t);
+        const float2 tauEtaU = fast_tau ? pdiv(tau2, lo2(ce), hi2(ce)) : make_float2(tau / -ce.x, tau / -ce.y);
+        const float4 cA = S.uvA(t);
+        const float2 cB = S.uvB(t);
+        const float2 ub = lo2(cA);
+        const float2 uT = kFuseUT ? pfma(tauEtaU, padd(gTx, gTy), ub) : padd(ub, pmul(tauEtaU, padd(gTx, gTy)));
+        const float2 d = psub(uT, u);
+        const float2 rho = kFuseRho ? pfma(iu, d, iz) : padd(pmul(iu, d), iz);
+        const float2 t1 = pmul(f2(kc.lambda), tauEtaU);
+        const float2 t2 = pmul(t1, iu);
+        const float2 bound = pmul(t2, iu);
+        const float4 cu = S.cU(t);
+        float2 qr = pdiv(rho, lo2(cu), hi2(cu));
+        if (!div_range(rho.x)) qr.x = rho.x / iu.x;
+        if (!div_range(rho.y)) qr.y = rho.y / iu.y;
+        const float2 dmid = psub(d, qr);
+        const float2 dlo = kFuseLo ? pfma(t1, iu, d) : padd(d, t2);
+        const float2 dhi = kFuseHi ? pfma(make_float2(-t1.x, -t1.y), iu, d) : psub(d, t2);
+        float2 du;
+        {
+          const float eps = 1E-7f;
+          const float mx = fabsf(iu.x) < eps ? d.x : dmid.x, my = fabsf(iu.y) < eps ? d.y : dmid.y;
+          du.x = (rho.x <= bound.x && rho.x >= -bound.x) ? mx
+                 : rho.x < -bound.x                      ? dlo.x
+                 : rho.x > bound.x                       ? dhi.x
+                                                         : 0.f;
+          du.y = (rho.y <= bound.y && rho.y >= -bound.y) ? my
+                 : rho.y < -bound.y                      ? dlo.y
+                 : rho.y > bound.y                       ? dhi.y
+                                                         : 0.f;
+        }
+        const float2 un = padd(u, du);
+        // updatePrimalVariables with all four neighbours unmasked (Python/vfs.cu:533-569)
+        const float4 qa = S.qA(t), qb = S.qB(t);
+        float4 qwa = S.qA(tW), qwb = S.qB(tW), qna = S.qA(tN), qnb = S.qB(tN);
+        if (seamW) qwa.y = qwa.x, qwb.w = qwb.z;
+        if (seamN) qna.w = qna.z, qnb.y = qnb.x;
+        const float2 gQx = psub(lo2(qa), lo2(qwa)), gQw = psub(hi2(qb), hi2(qwb));
+        const float2 gQy = psub(hi2(qa), hi2(qna)), gQz = psub(lo2(qb), lo2(qnb));
+        const float2 tux = pfma(ra, px, pmul(rc, py)), tuy = pfma(rc, px, pmul(rb, py));
+        const float4 cy = S.cY(t), cz = S.cZ(t);
+        const float2 te1 = fast_tau ? pdiv(tau2, lo2(cy), hi2(cy)) : make_float2(tau / -cy.x, tau / -cy.y);
+        const float2 te2 = fast_tau ? pdiv(tau2, lo2(cz), hi2(cz)) : make_float2(tau / -cz.x, tau / -cz.y);
+        const float2 vbx = hi2(cA), vby = cB;
+        const float2 Vx = pfma(te1, pfma(f2(kc.alpha1), tux, pmul(f2(kc.alpha0), padd(gQx, gQz))), vbx);
+        const float2 Vy = pfma(te2, pfma(f2(kc.alpha1), tuy, pmul(f2(kc.alpha0), padd(gQw, gQy))), vby);
+        const float2 uo = pfma(f2(mu), psub(un, ub), un);
+        const float2 vxo = pfma(f2(mu), psub(Vx, vbx), Vx), vyo = pfma(f2(mu), psub(Vy, vby), Vy);
+        u = un;
+        S.uvA(t) = make_float4(uo.x, uo.y, vxo.x, vxo.y);
+        S.uvB(t) = vyo;
+      } else if (cl == 1) {
+        u = f2(0.f);
+        S.uvA(t) = make_float4(0.f, 0.f, 0.f, 0.f);
+        S.uvB(t) = f2(0.f);
+      } else {
+#pragma unroll 1
+        for (int j = 0; j < 2; ++j) {
+          if (2 * s > (int)(info >> (16 + 8 * j) & 63u)) continue;
+          const int e = j ? e1 : e0;
+          const uint8_t cd = (uint8_t)(info >> (8 * j) & 31u);
+          float un = 0.f, uo = 0.f;
+          float2 vo = make_float2(0.f, 0.f);
+          if (cd & kSelf) {
+            // eta' (the records hold -eta') gives the reference's result:
+            // where |eta| < eps, eta' = 1 and tau / 1 == tau
+            const float exj = -S.at(fCE, e, 0), eyj = -S.at(fCY, e, 0), ezj = -S.at(fCZ, e, 0);
+            const float ub = S.at(fUVA, e, 0);
+            const float2 vb = make_float2(S.at(fUVA, e, 1), S.at(fUVB, e, 0));
+            un = threshold_px(cd, tau, make_float2(S.at(fTP, e, 0), S.at(fTP, e, 1)),
+                              make_float2(S.at(fTP, e - 1, 0), 0.f), make_float2(0.f, S.at(fTP, e - WX, 1)),
+                              j ? u.y : u.x, ub, make_float2(j ? iu.y : iu.x, j ? iz.y : iz.x), exj, kc.lambda);
+            const float4 qc = make_float4(S.at(fQA, e, 0), S.at(fQA, e, 1), S.at(fQB, e, 0), S.at(fQB, e, 1));
+            const float4 qW = make_float4(S.at(fQA, e - 1, 0), 0.f, 0.f, S.at(fQB, e - 1, 1));
+            const float4 qN = make_float4(0.f, S.at(fQA, e - WX, 1), S.at(fQB, e - WX, 0), 0.f);
+            primal_px(cd, tau, mu, j ? make_float2(px.y, py.y) : make_float2(px.x, py.x), qc, qW, qN, un, ub, vb,
+                      make_float3(j ? ra.y : ra.x, j ? rb.y : rb.x, j ? rc.y : rc.x), make_float3(exj, eyj, ezj),
+                      kc.alpha0, kc.alpha1, &uo, &vo);
+          }
+          if (j) u.y = un;
+          else u.x = un;
+          S.at(fUVA, e, 0) = uo;
+          S.at(fUVA, e, 1) = vo.x;
+          S.at(fUVB, e, 0) = vo.y;
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- write back the tile (real pixels only)
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int e = j ? e1 : e0;
+    const int wy = e / WX, wx = e - wy * WX;
+    const int tx = wx - 2 * K, ty = wy - 2 * K;
+    if (e >= N || tx < 0 || tx >= TX || ty < 0 || ty >= TY) continue;
+    const int X = x0 + tx, Y = y0 + ty;
+    if (X >= w || Y >= h) continue;
+    const long f = (long)Y * w + X;
+    out.u[f] = j ? u.y : u.x;
+    out.ub[f] = S.at(fUVA, e, 0);
+    out.vbx[f] = S.at(fUVA, e, 1);
+    out.vby[f] = S.at(fUVB, e, 0);
+    out.px[f] = j ? px.y : px.x;
+    out.py[f] = j ? py.y : py.x;
+    out.qx[f] = S.at(fQA, e, 0);
+    out.qy[f] = S.at(fQA, e, 1);
+    out.qz[f] = S.at(fQB, e, 0);
+    out.qw[f] = S.at(fQB, e, 1);
+  }
+}
+
+template <int K, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, 1)
+    k_tgv_pair(TgvState in, TgvState out, TgvConsts cst, const float3* __restrict__ sched, int it0, int niter,
+               SolverConsts kc, int h, int w) {
+  tgv_pair_tile<K, TX, TY, NT>(in, out, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY);
+}
+
+// Batched: one launch over the tiles of many images (see k_tgv_reg_batch).
+template <int K, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, 1)
+    k_tgv_pair_batch(const TgvBatchItem* __restrict__ items, int n_items, int parity,
+                     const float3* __restrict__ sched, int it0, int niter, SolverConsts kc) {
+  int lo = 0, hi = n_items - 1;
+  const int bid = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].tile_base <= bid) lo = mid;
+    else hi = mid - 1;
+  }
+  const TgvBatchItem& it = items[lo];
+  const int t = bid - it.tile_base;
+  const int ty = t / it.tiles_x, tx = t - ty * it.tiles_x;
+  tgv_pair_tile<K, TX, TY, NT>(it.st[parity], it.st[parity ^ 1], it.cst, sched, it0, niter, kc, it.h, it.w, tx * TX,
+                               ty * TY);
+}
+
+}  // namespace
+}  // namespace vfs
