@@ -43,19 +43,20 @@ def _reference(prm, p, tvf, cvf):
     return flow, xyz
 
 
-def _check(p, want, got, what, min_depth_frac=0.5):
+def _check(p, want, got, what):
     (rf, rx), (of, ox) = want, got
     assert rf.shape == of.shape and rx.shape == ox.shape
     df = np.count_nonzero(np.ascontiguousarray(rf).view(np.uint32) != np.ascontiguousarray(of).view(np.uint32))
     dx = np.count_nonzero(np.ascontiguousarray(rx).view(np.uint32) != np.ascontiguousarray(ox).view(np.uint32))
     zr, zo = rx[..., 2].astype(np.float64), ox[..., 2].astype(np.float64)
+    assert df == 0, f"{what}: {df} of {rf.size} flow values differ from the reference kernels"
+    assert dx == 0, f"{what}: {dx} of {rx.size} xyz values differ from the reference kernels"
+    # at Lambda 50 the method drifts from the true depth, so only part of the
+    # mask has a plausible reference depth (29-41 % at 800^2 and 512^2)
     sel = (p.mask != 0) & np.isfinite(zr) & (zr > 0) & (zr <= 100)
-    assert sel.sum() >= min_depth_frac * np.count_nonzero(p.mask)
     if sel.any():
         err = np.median(np.abs(zo[sel] - zr[sel]) / zr[sel])
         assert err <= DEPTH_TOL, f"{what}: median relative depth error {err}"
-    assert df == 0, f"{what}: {df} of {rf.size} flow values differ from the reference kernels"
-    assert dx == 0, f"{what}: {dx} of {rx.size} xyz values differ from the reference kernels"
 
 
 def _drop_in(prm, p, tvf, cvf):
@@ -126,7 +127,4 @@ def test_parity_uneven_batch_subset(gpu):
         xyz = batch.triangulate(i, cam, p.t).cpu().numpy()
         side = p.img_ref.shape[0]
         want = _reference(bench_params(side, side, n_level=4, n_warp=10, n_iter=50), p, tvf, cvf)
-        # the reference's triangulation uses t.x and t.z only (Python/vfs.cu:729-734): with a random
-        # translation direction its depth is often not finite or negative, so no minimum share is asked
-        _check(p, want, (flows[i], xyz), f"batched pair {i} ({side}x{side}, t {np.round(work[i][1], 3)})",
-               min_depth_frac=0.0)
+        _check(p, want, (flows[i], xyz), f"batched pair {i} ({side}x{side}, t {np.round(work[i][1], 3)})")
