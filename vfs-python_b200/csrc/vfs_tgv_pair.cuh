@@ -52,17 +52,15 @@ __device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b
 __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
-// RN(x / y) of both lanes from ny = -y and r = RN(1 / y) (see the file
-// comment); a lane whose result is NaN is divided with '/'.
+// RN(x / y) of both lanes from ny = -y and r = RN(1 / y), for x and y in
+// the reciprocal range (see the file comment); the callers route other
+// operands to '/'.
 __device__ __forceinline__ float2 pdiv(float2 x, float2 ny, float2 r) {
   const float2 q0 = pmul(x, r);
   const float2 e0 = pfma(q0, ny, x);
   const float2 q1 = pfma(e0, r, q0);
   const float2 e1 = pfma(q1, ny, x);
-  float2 q = pfma(e1, r, q1);
-  if (q.x != q.x) q.x = x.x / -ny.x;
-  if (q.y != q.y) q.y = x.y / -ny.y;
-  return q;
+  return pfma(e1, r, q1);
 }
 
 // How the reference's threshold step rounds its multiply-adds (the compiler
@@ -100,16 +98,7 @@ struct PairSmem {
   __device__ __forceinline__ float4& cZ(int t) const { return base[7 * NT + t]; }
   __device__ __forceinline__ float4& cU(int t) const { return base[8 * NT + t]; }
   static constexpr int kRecords = 9;
-  // scalar view of window pixel e: component c of a record family whose
-  // records hold two components (c = 0, 1) per lane
-  __device__ __forceinline__ float& at(int family, int e, int c) const {
-    const int lane = e >= NT;
-    const int t = e - lane * NT;
-    return reinterpret_cast<float*>(base + family * NT + t)[2 * c + lane];
-  }
 };
-
-enum PairFamily { fUVA = 0, fUVB = 1, fQA = 2, fQB = 3, fTP = 4, fCE = 5, fCY = 6, fCZ = 7 };
 
 template <int K, int TX, int TY>
 constexpr size_t pair_smem_bytes(int nt) {
@@ -130,6 +119,84 @@ __device__ __forceinline__ int last_phase(int wx, int wy, int k) {
     if (wx >= lo_p && wx < hiX && wy >= lo_p && wy < hiY) last = 2 * s;
   }
   return last;
+}
+
+// The dual step lane by lane with the scalar per-pixel function (pixels
+// that are masked or beside masked ones), reading the pair records of the
+// thread and its four neighbours.  Out of line, so that its registers do not
+// weigh on the packed path.
+template <int NT, int WX>
+__device__ __noinline__ void pair_dual_lanes(const PairSmem<NT> S, int t, unsigned info, float2 ra, float2 rb, float2 rc,
+                                             float scaleP, float scaleQ, float2& px, float2& py, float2& tpx,
+                                             float2& tpy, float2& qx, float2& qy, float2& qz, float2& qw) {
+  const bool seamE = t + 1 == NT, seamS = t + WX >= NT, seamW = t == 0, seamN = t < WX;
+  const int tE = seamE ? 0 : t + 1, tS = seamS ? t + WX - NT : t + WX;
+  const int tW = seamW ? NT - 1 : t - 1, tN = seamN ? t + NT - WX : t - WX;
+  auto uv_lane = [&](int r, int lane) {
+    const float4 a = S.uvA(r);
+    const float2 b = S.uvB(r);
+    return lane ? make_float3(a.y, a.w, b.y) : make_float3(a.x, a.z, b.x);
+  };
+#pragma unroll 1
+  for (int j = 0; j < 2; ++j) {
+    const uint8_t cd = (uint8_t)(info >> (8 * j) & 31u);
+    float2 p = make_float2(j ? px.y : px.x, j ? py.y : py.x), tp = make_float2(0.f, 0.f);
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (cd & kSelf) {
+      const int lE = seamE ? 1 : j, lS = seamS ? 1 : j, lW = seamW ? 0 : j, lN = seamN ? 0 : j;
+      const float3 c = uv_lane(t, j), cE = uv_lane(tE, lE), cW = uv_lane(tW, lW);
+      const float3 cS = uv_lane(tS, lS), cN = uv_lane(tN, lN);
+      const float4 qa = S.qA(t), qb = S.qB(t);
+      q = j ? make_float4(qa.y, qa.w, qb.y, qb.w) : make_float4(qa.x, qa.z, qb.x, qb.z);
+      dual_px(cd, c.x, make_float2(c.y, c.z), cE.x, make_float2(cE.y, cE.z), cW.x, make_float2(cW.y, cW.z), cS.x,
+              make_float2(cS.y, cS.z), cN.x, make_float2(cN.y, cN.z),
+              j ? make_float3(ra.y, rb.y, rc.y) : make_float3(ra.x, rb.x, rc.x), scaleP, scaleQ, &p, &tp, &q);
+    } else {
+      p = make_float2(0.f, 0.f);
+    }
+    if (j) px.y = p.x, py.y = p.y, tpx.y = tp.x, tpy.y = tp.y, qx.y = q.x, qy.y = q.y, qz.y = q.z, qw.y = q.w;
+    else px.x = p.x, py.x = p.y, tpx.x = tp.x, tpy.x = tp.y, qx.x = q.x, qy.x = q.y, qz.x = q.z, qw.x = q.w;
+  }
+}
+
+// The threshold and primal steps lane by lane (see pair_dual_lanes).
+template <int NT, int WX>
+__device__ __noinline__ void pair_primal_lanes(const PairSmem<NT> S, int t, unsigned info, float2 ra, float2 rb,
+                                               float2 rc, float2 iu, float2 iz, float2 u, float2 px, float2 py,
+                                               float tau, float mu, float lambda, float alpha0, float alpha1,
+                                               float2& un, float2& uo, float2& vxo, float2& vyo) {
+  const bool seamW = t == 0, seamN = t < WX;
+  const int tW = seamW ? NT - 1 : t - 1, tN = seamN ? t + NT - WX : t - WX;
+  auto rec_lane = [](float4 r, int lane) { return lane ? r.y : r.x; };
+  auto rec_lane2 = [](float4 r, int lane) { return lane ? r.w : r.z; };
+#pragma unroll 1
+  for (int j = 0; j < 2; ++j) {
+    const uint8_t cd = (uint8_t)(info >> (8 * j) & 31u);
+    float unj = 0.f, uoj = 0.f;
+    float2 vo = make_float2(0.f, 0.f);
+    if (cd & kSelf) {
+      const int lW = seamW ? 0 : j, lN = seamN ? 0 : j;
+      // eta' (the records hold -eta') gives the reference's result: where
+      // |eta| < eps, eta' = 1 and tau / 1 == tau
+      const float3 eta = make_float3(-rec_lane(S.cE(t), j), -rec_lane(S.cY(t), j), -rec_lane(S.cZ(t), j));
+      const float4 tc = S.tp(t), tw = S.tp(tW), tn = S.tp(tN);
+      const float4 ua = S.uvA(t);
+      const float2 ubb = S.uvB(t);
+      const float ub = rec_lane(ua, j);
+      const float2 vb = make_float2(rec_lane2(ua, j), j ? ubb.y : ubb.x);
+      unj = threshold_px(cd, tau, make_float2(rec_lane(tc, j), rec_lane2(tc, j)), make_float2(rec_lane(tw, lW), 0.f),
+                         make_float2(0.f, rec_lane2(tn, lN)), j ? u.y : u.x, ub,
+                         j ? make_float2(iu.y, iz.y) : make_float2(iu.x, iz.x), eta.x, lambda);
+      const float4 qa = S.qA(t), qb = S.qB(t), qwa = S.qA(tW), qwb = S.qB(tW), qna = S.qA(tN), qnb = S.qB(tN);
+      primal_px(cd, tau, mu, j ? make_float2(px.y, py.y) : make_float2(px.x, py.x),
+                make_float4(rec_lane(qa, j), rec_lane2(qa, j), rec_lane(qb, j), rec_lane2(qb, j)),
+                make_float4(rec_lane(qwa, lW), 0.f, 0.f, rec_lane2(qwb, lW)),
+                make_float4(0.f, rec_lane2(qna, lN), rec_lane(qnb, lN), 0.f), unj, ub, vb,
+                j ? make_float3(ra.y, rb.y, rc.y) : make_float3(ra.x, rb.x, rc.x), eta, alpha0, alpha1, &uoj, &vo);
+    }
+    if (j) un.y = unj, uo.y = uoj, vxo.y = vo.x, vyo.y = vo.y;
+    else un.x = unj, uo.x = uoj, vxo.x = vo.x, vyo.x = vo.y;
+  }
 }
 
 template <int K, int TX, int TY, int NT>
@@ -162,7 +229,9 @@ __device__ __forceinline__ void tgv_pair_tile(const TgvState& in, const TgvState
 
   // ---- per-warp constants of both pixels
   float2 ra, rb, rc, iu, iz;
-  int code[2], last[2];
+  int code[2];
+  int lastP = 0;    // the last phase either pixel takes part in
+  bool fdiv = true;  // the reciprocal divisions of the packed path hold for both pixels
   {
     float4 rcp[2];
     float ex[2], ey[2], ez[2];
@@ -177,26 +246,32 @@ __device__ __forceinline__ void tgv_pair_tile(const TgvState& in, const TgvState
       const float du = ok ? cst.iu[f] : 0.f, dz = ok ? cst.iz[f] : 0.f;
       if (j) ra.y = a, rb.y = b, rc.y = c, iu.y = du, iz.y = dz;
       else ra.x = a, rb.x = b, rc.x = c, iu.x = du, iz.x = dz;
-      ex[j] = ok ? cst.ex[f] : 1.f;
-      ey[j] = ok ? cst.ey[f] : 1.f;
-      ez[j] = ok ? cst.ez[f] : 1.f;
+      ex[j] = eta_used(ok ? cst.ex[f] : 1.f);
+      ey[j] = eta_used(ok ? cst.ey[f] : 1.f);
+      ez[j] = eta_used(ok ? cst.ez[f] : 1.f);
       // without reciprocal records every division takes '/' (NaN reciprocals)
       rcp[j] = ok && cst.rcp ? cst.rcp[f] : make_float4(nan, nan, nan, nan);
       code[j] = ok ? cst.code[f] : 0;
-      last[j] = e < N ? last_phase<K, TX, TY>(wx, wy, k) : 0;
+      if (e < N) lastP = max(lastP, last_phase<K, TX, TY>(wx, wy, k));
+      // every eta in the reciprocal range with its reciprocal formed (NaN
+      // otherwise), and dIu too unless the reference never divides by it
+      fdiv = fdiv && div_range(ex[j]) && div_range(ey[j]) && div_range(ez[j]) && rcp[j].x == rcp[j].x &&
+             rcp[j].y == rcp[j].y && rcp[j].z == rcp[j].z &&
+             (fabsf(du) < 1E-7f || (div_range(du) && rcp[j].w == rcp[j].w));
     }
-    S.cE(t) = make_float4(-eta_used(ex[0]), -eta_used(ex[1]), rcp[0].x, rcp[1].x);
-    S.cY(t) = make_float4(-eta_used(ey[0]), -eta_used(ey[1]), rcp[0].y, rcp[1].y);
-    S.cZ(t) = make_float4(-eta_used(ez[0]), -eta_used(ez[1]), rcp[0].z, rcp[1].z);
+    S.cE(t) = make_float4(-ex[0], -ex[1], rcp[0].x, rcp[1].x);
+    S.cY(t) = make_float4(-ey[0], -ey[1], rcp[0].y, rcp[1].y);
+    S.cZ(t) = make_float4(-ez[0], -ez[1], rcp[0].z, rcp[1].z);
     S.cU(t) = make_float4(-iu.x, -iu.y, rcp[0].w, rcp[1].w);
   }
-  // class 0: both pixels unmasked with all four neighbours unmasked (packed
-  // path); 1: both masked (zero state); 2: lane by lane.  info bits 0-4 /
-  // 8-12: the mask codes, 16-21 / 24-29: the last phases, 30-31: the class.
-  const unsigned cls =
-      (code[0] == 0x1F && code[1] == 0x1F) ? 0u : (!(code[0] & kSelf) && !(code[1] & kSelf)) ? 1u : 2u;
-  const unsigned info = (unsigned)code[0] | (unsigned)code[1] << 8 | (unsigned)last[0] << 16 |
-                        (unsigned)last[1] << 24 | cls << 30;
+  // class 0: both pixels unmasked with all four neighbours unmasked and
+  // their divisors in the reciprocal range (packed path); 1: both masked
+  // (zero state); 2: lane by lane with the scalar per-pixel functions.
+  // info bits 0-4 / 8-12: the mask codes, 16-21: the last phase, 30-31: the class.
+  const unsigned cls = (code[0] == 0x1F && code[1] == 0x1F && fdiv) ? 0u
+                       : (!(code[0] & kSelf) && !(code[1] & kSelf)) ? 1u
+                                                                     : 2u;
+  const unsigned info = (unsigned)code[0] | (unsigned)code[1] << 8 | (unsigned)lastP << 16 | cls << 30;
 
   // a tile whose pixels are all masked ends with zero state (masked pixels
   // are written 0 every iteration): write that and skip the iterations
@@ -258,198 +333,165 @@ __device__ __forceinline__ void tgv_pair_tile(const TgvState& in, const TgvState
   }
   __syncthreads();
 
+  // the bar variables (u_, v_) of a pair record, and across the seam the
+  // other lane of the neighbour's record (see the file comment)
+  struct UV {
+    float2 u, vx, vy;
+  };
+  auto ld_uv = [&](int r) {
+    const float4 a = S.uvA(r);
+    return UV{lo2(a), hi2(a), S.uvB(r)};
+  };
+  auto lane_y_to_x = [](UV& v) { v.u.x = v.u.y, v.vx.x = v.vx.y, v.vy.x = v.vy.y; };
+  // (recomputed where used: cheaper than keeping them in registers)
+#define VFS_PAIR_NEIGHBOURS                                                              \
+  const bool seamE = t + 1 == NT, seamS = t + WX >= NT, seamW = t == 0, seamN = t < WX; \
+  const int tE = seamE ? 0 : t + 1, tS = seamS ? t + WX - NT : t + WX;                  \
+  const int tW = seamW ? NT - 1 : t - 1, tN = seamN ? t + NT - WX : t - WX;             \
+  (void)tE, (void)tS, (void)tW, (void)tN;
+  const unsigned cl = info >> 30;
+  const int lastPh = (int)(info >> 16 & 63u);
+
   for (int s = 1; s <= k; ++s) {
     const float* const sc = sSch + 5 * (s - 1);
     const float tau = sc[1], mu = sc[2];
     const float scaleP = sc[3], scaleQ = sc[4];  // alpha1 sigma / etaP, alpha0 sigma / etaQ
-    const unsigned cl = info >> 30;
-    const int lastP = max((int)(info >> 16 & 63u), (int)(info >> 24 & 63u));
     // ---------------------------------------------------------------- dual step
-    if (2 * s - 1 <= lastP) {
-      if (cl == 0) {
-        // neighbour records E and S, across the seam the other lane
-        const bool seamE = t + 1 == NT, seamS = t + WX >= NT;
-        const int tE = seamE ? 0 : t + 1, tS = seamS ? t + WX - NT : t + WX;
-        const float4 cA = S.uvA(t);
-        const float2 cB = S.uvB(t);
-        float4 eA = S.uvA(tE);
-        float2 eB = S.uvB(tE);
-        float4 sA = S.uvA(tS);
-        float2 sB = S.uvB(tS);
-        if (seamE) eA.x = eA.y, eA.z = eA.w, eB.x = eB.y;
-        if (seamS) sA.x = sA.y, sA.z = sA.w, sB.x = sB.y;
-        const float2 uc = lo2(cA), vcx = hi2(cA), vcy = cB;
-        // updateDualVariables with E and S unmasked (Python/vfs.cu:352-408)
-        const float2 gUx = psub(psub(lo2(eA), uc), vcx);
-        const float2 gVx = psub(hi2(eA), vcx), gVw = psub(eB, vcy);
-        const float2 gUy = psub(psub(lo2(sA), uc), vcy);
-        const float2 gVy = psub(sB, vcy), gVz = psub(hi2(sA), vcx);
-        const float2 tux = pfma(ra, gUx, pmul(rc, gUy)), tuy = pfma(rc, gUx, pmul(rb, gUy));
-        float2 upx = pfma(f2(scaleP), tux, px), upy = pfma(f2(scaleP), tuy, py);
-        // projection onto the unit ball: a lane with |up|^2 < 0.98 has a norm
-        // below 1, so max(hypot, 1) is 1 and up / 1 == up; others as the reference
-        const float2 n2 = pfma(upx, upx, pmul(upy, upy));
-        if (!(n2.x < 0.98f)) {
-          const float nr = fmaxf(hypotf(upx.x, upy.x), 1.0f);
-          upx.x = upx.x / nr, upy.x = upy.x / nr;
-        }
-        if (!(n2.y < 0.98f)) {
-          const float nr = fmaxf(hypotf(upx.y, upy.y), 1.0f);
-          upx.y = upx.y / nr, upy.y = upy.y / nr;
-        }
-        px = upx, py = upy;
-        const float2 tpx = pfma(ra, upx, pmul(rc, upy)), tpy = pfma(rc, upx, pmul(rb, upy));
-        S.tp(t) = make_float4(tpx.x, tpx.y, tpy.x, tpy.y);
-        const float4 qa = S.qA(t), qb = S.qB(t);
-        float2 qx = pfma(f2(scaleQ), gVx, lo2(qa)), qy = pfma(f2(scaleQ), gVy, hi2(qa));
-        float2 qz = pfma(f2(scaleQ), gVz, lo2(qb)), qw = pfma(f2(scaleQ), gVw, hi2(qb));
-        const float2 m2 = pfma(qx, qx, pfma(qy, qy, pfma(qz, qz, pmul(qw, qw))));
-        if (!(m2.x < 0.98f)) {
-          const float nr = fmaxf(norm4df(qx.x, qy.x, qz.x, qw.x), 1.0f);
-          qx.x = qx.x / nr, qy.x = qy.x / nr, qz.x = qz.x / nr, qw.x = qw.x / nr;
-        }
-        if (!(m2.y < 0.98f)) {
-          const float nr = fmaxf(norm4df(qx.y, qy.y, qz.y, qw.y), 1.0f);
-          qx.y = qx.y / nr, qy.y = qy.y / nr, qz.y = qz.y / nr, qw.y = qw.y / nr;
-        }
-        S.qA(t) = make_float4(qx.x, qx.y, qy.x, qy.y);
-        S.qB(t) = make_float4(qz.x, qz.y, qw.x, qw.y);
-      } else if (cl == 1) {
+    if (2 * s - 1 <= lastPh) {
+      if (cl == 1) {
         px = py = f2(0.f);
         S.tp(t) = make_float4(0.f, 0.f, 0.f, 0.f);
         S.qA(t) = S.qB(t) = make_float4(0.f, 0.f, 0.f, 0.f);
       } else {
-#pragma unroll 1
-        for (int j = 0; j < 2; ++j) {
-          if (2 * s - 1 > (int)(info >> (16 + 8 * j) & 63u)) continue;
-          const int e = j ? e1 : e0;
-          const uint8_t cd = (uint8_t)(info >> (8 * j) & 31u);
-          float2 p = j ? make_float2(px.y, py.y) : make_float2(px.x, py.x), tp = make_float2(0.f, 0.f);
-          float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (cd & kSelf) {
-            q = make_float4(S.at(fQA, e, 0), S.at(fQA, e, 1), S.at(fQB, e, 0), S.at(fQB, e, 1));
-            auto uv = [&](int i) { return make_float3(S.at(fUVA, i, 0), S.at(fUVA, i, 1), S.at(fUVB, i, 0)); };
-            const float3 c = uv(e), cE = uv(e + 1), cW = uv(e - 1), cS = uv(e + WX), cN = uv(e - WX);
-            dual_px(cd, c.x, make_float2(c.y, c.z), cE.x, make_float2(cE.y, cE.z), cW.x, make_float2(cW.y, cW.z),
-                    cS.x, make_float2(cS.y, cS.z), cN.x, make_float2(cN.y, cN.z),
-                    make_float3(j ? ra.y : ra.x, j ? rb.y : rb.x, j ? rc.y : rc.x), scaleP, scaleQ, &p, &tp, &q);
-          } else {
-            p = make_float2(0.f, 0.f);
+        VFS_PAIR_NEIGHBOURS
+        float2 tpx, tpy, qx, qy, qz, qw;
+        if (cl == 0) {
+          UV c = ld_uv(t), cE = ld_uv(tE), cS = ld_uv(tS);
+          if (seamE) lane_y_to_x(cE);
+          if (seamS) lane_y_to_x(cS);
+          const float4 qa = S.qA(t), qb = S.qB(t);
+          // updateDualVariables with E and S unmasked (Python/vfs.cu:352-408)
+          const float2 gUx = psub(psub(cE.u, c.u), c.vx);
+          const float2 gVx = psub(cE.vx, c.vx), gVw = psub(cE.vy, c.vy);
+          const float2 gUy = psub(psub(cS.u, c.u), c.vy);
+          const float2 gVy = psub(cS.vy, c.vy), gVz = psub(cS.vx, c.vx);
+          const float2 tux = pfma(ra, gUx, pmul(rc, gUy)), tuy = pfma(rc, gUx, pmul(rb, gUy));
+          float2 upx = pfma(f2(scaleP), tux, px), upy = pfma(f2(scaleP), tuy, py);
+          // projection onto the unit ball: a lane with |up|^2 < 0.98 has a norm
+          // below 1, so max(hypot, 1) is 1 and up / 1 == up; others as the reference
+          const float2 n2 = pfma(upx, upx, pmul(upy, upy));
+          if (!(n2.x < 0.98f)) {
+            const float nr = fmaxf(hypotf(upx.x, upy.x), 1.0f);
+            upx.x = upx.x / nr, upy.x = upy.x / nr;
           }
-          if (j) px.y = p.x, py.y = p.y;
-          else px.x = p.x, py.x = p.y;
-          S.at(fTP, e, 0) = tp.x;
-          S.at(fTP, e, 1) = tp.y;
-          S.at(fQA, e, 0) = q.x;
-          S.at(fQA, e, 1) = q.y;
-          S.at(fQB, e, 0) = q.z;
-          S.at(fQB, e, 1) = q.w;
+          if (!(n2.y < 0.98f)) {
+            const float nr = fmaxf(hypotf(upx.y, upy.y), 1.0f);
+            upx.y = upx.y / nr, upy.y = upy.y / nr;
+          }
+          px = upx, py = upy;
+          tpx = pfma(ra, upx, pmul(rc, upy)), tpy = pfma(rc, upx, pmul(rb, upy));
+          qx = pfma(f2(scaleQ), gVx, lo2(qa)), qy = pfma(f2(scaleQ), gVy, hi2(qa));
+          qz = pfma(f2(scaleQ), gVz, lo2(qb)), qw = pfma(f2(scaleQ), gVw, hi2(qb));
+          const float2 m2 = pfma(qx, qx, pfma(qy, qy, pfma(qz, qz, pmul(qw, qw))));
+          if (!(m2.x < 0.98f)) {
+            const float nr = fmaxf(norm4df(qx.x, qy.x, qz.x, qw.x), 1.0f);
+            qx.x = qx.x / nr, qy.x = qy.x / nr, qz.x = qz.x / nr, qw.x = qw.x / nr;
+          }
+          if (!(m2.y < 0.98f)) {
+            const float nr = fmaxf(norm4df(qx.y, qy.y, qz.y, qw.y), 1.0f);
+            qx.y = qx.y / nr, qy.y = qy.y / nr, qz.y = qz.y / nr, qw.y = qw.y / nr;
+          }
+        } else {
+          // lane by lane with the scalar step: masked pixels and pixels
+          // beside masked ones (out of line: its registers stay off the packed path)
+          pair_dual_lanes<NT, WX>(S, t, info, ra, rb, rc, scaleP, scaleQ, px, py, tpx, tpy, qx, qy, qz, qw);
         }
+        S.tp(t) = make_float4(tpx.x, tpx.y, tpy.x, tpy.y);
+        S.qA(t) = make_float4(qx.x, qx.y, qy.x, qy.y);
+        S.qB(t) = make_float4(qz.x, qz.y, qw.x, qw.y);
       }
     }
     __syncthreads();
     // ------------------------------------------------- threshold + primal steps
-    if (2 * s <= lastP) {
-      if (cl == 0) {
-        const bool seamW = t == 0, seamN = t < WX;
-        const int tW = seamW ? NT - 1 : t - 1, tN = seamN ? t + NT - WX : t - WX;
-        const bool fast_tau = div_range(tau);
-        const float2 tau2 = f2(tau);
-        // l1Thresholding with all four neighbours unmasked (Python/vfs.cu:444-494)
-        const float4 tc = S.tp(t);
-        float4 tw = S.tp(tW), tn = S.tp(tN);
-        if (seamW) tw.y = tw.x;
-        if (seamN) tn.w = tn.z;
-        const float2 gTx = psub(lo2(tc), lo2(tw)), gTy = psub(hi2(tc), hi2(tn));
-        const float4 ce = S.cE(t);
-        const float2 tauEtaU = fast_tau ? pdiv(tau2, lo2(ce), hi2(ce)) : make_float2(tau / -ce.x, tau / -ce.y);
-        const float4 cA = S.uvA(t);
-        const float2 cB = S.uvB(t);
-        const float2 ub = lo2(cA);
-        const float2 uT = kFuseUT ? pfma(tauEtaU, padd(gTx, gTy), ub) : padd(ub, pmul(tauEtaU, padd(gTx, gTy)));
-        const float2 d = psub(uT, u);
-        const float2 rho = kFuseRho ? pfma(iu, d, iz) : padd(pmul(iu, d), iz);
-        const float2 t1 = pmul(f2(kc.lambda), tauEtaU);
-        const float2 t2 = pmul(t1, iu);
-        const float2 bound = pmul(t2, iu);
-        const float4 cu = S.cU(t);
-        float2 qr = pdiv(rho, lo2(cu), hi2(cu));
-        if (!div_range(rho.x)) qr.x = rho.x / iu.x;
-        if (!div_range(rho.y)) qr.y = rho.y / iu.y;
-        const float2 dmid = psub(d, qr);
-        const float2 dlo = kFuseLo ? pfma(t1, iu, d) : padd(d, t2);
-        const float2 dhi = kFuseHi ? pfma(make_float2(-t1.x, -t1.y), iu, d) : psub(d, t2);
-        float2 du;
-        {
-          const float eps = 1E-7f;
-          const float mx = fabsf(iu.x) < eps ? d.x : dmid.x, my = fabsf(iu.y) < eps ? d.y : dmid.y;
-          du.x = (rho.x <= bound.x && rho.x >= -bound.x) ? mx
-                 : rho.x < -bound.x                      ? dlo.x
-                 : rho.x > bound.x                       ? dhi.x
-                                                         : 0.f;
-          du.y = (rho.y <= bound.y && rho.y >= -bound.y) ? my
-                 : rho.y < -bound.y                      ? dlo.y
-                 : rho.y > bound.y                       ? dhi.y
-                                                         : 0.f;
-        }
-        const float2 un = padd(u, du);
-        // updatePrimalVariables with all four neighbours unmasked (Python/vfs.cu:533-569)
-        const float4 qa = S.qA(t), qb = S.qB(t);
-        float4 qwa = S.qA(tW), qwb = S.qB(tW), qna = S.qA(tN), qnb = S.qB(tN);
-        if (seamW) qwa.y = qwa.x, qwb.w = qwb.z;
-        if (seamN) qna.w = qna.z, qnb.y = qnb.x;
-        const float2 gQx = psub(lo2(qa), lo2(qwa)), gQw = psub(hi2(qb), hi2(qwb));
-        const float2 gQy = psub(hi2(qa), hi2(qna)), gQz = psub(lo2(qb), lo2(qnb));
-        const float2 tux = pfma(ra, px, pmul(rc, py)), tuy = pfma(rc, px, pmul(rb, py));
-        const float4 cy = S.cY(t), cz = S.cZ(t);
-        const float2 te1 = fast_tau ? pdiv(tau2, lo2(cy), hi2(cy)) : make_float2(tau / -cy.x, tau / -cy.y);
-        const float2 te2 = fast_tau ? pdiv(tau2, lo2(cz), hi2(cz)) : make_float2(tau / -cz.x, tau / -cz.y);
-        const float2 vbx = hi2(cA), vby = cB;
-        const float2 Vx = pfma(te1, pfma(f2(kc.alpha1), tux, pmul(f2(kc.alpha0), padd(gQx, gQz))), vbx);
-        const float2 Vy = pfma(te2, pfma(f2(kc.alpha1), tuy, pmul(f2(kc.alpha0), padd(gQw, gQy))), vby);
-        const float2 uo = pfma(f2(mu), psub(un, ub), un);
-        const float2 vxo = pfma(f2(mu), psub(Vx, vbx), Vx), vyo = pfma(f2(mu), psub(Vy, vby), Vy);
-        u = un;
-        S.uvA(t) = make_float4(uo.x, uo.y, vxo.x, vxo.y);
-        S.uvB(t) = vyo;
-      } else if (cl == 1) {
+    if (2 * s <= lastPh) {
+      if (cl == 1) {
         u = f2(0.f);
         S.uvA(t) = make_float4(0.f, 0.f, 0.f, 0.f);
         S.uvB(t) = f2(0.f);
       } else {
-#pragma unroll 1
-        for (int j = 0; j < 2; ++j) {
-          if (2 * s > (int)(info >> (16 + 8 * j) & 63u)) continue;
-          const int e = j ? e1 : e0;
-          const uint8_t cd = (uint8_t)(info >> (8 * j) & 31u);
-          float un = 0.f, uo = 0.f;
-          float2 vo = make_float2(0.f, 0.f);
-          if (cd & kSelf) {
-            // eta' (the records hold -eta') gives the reference's result:
-            // where |eta| < eps, eta' = 1 and tau / 1 == tau
-            const float exj = -S.at(fCE, e, 0), eyj = -S.at(fCY, e, 0), ezj = -S.at(fCZ, e, 0);
-            const float ub = S.at(fUVA, e, 0);
-            const float2 vb = make_float2(S.at(fUVA, e, 1), S.at(fUVB, e, 0));
-            un = threshold_px(cd, tau, make_float2(S.at(fTP, e, 0), S.at(fTP, e, 1)),
-                              make_float2(S.at(fTP, e - 1, 0), 0.f), make_float2(0.f, S.at(fTP, e - WX, 1)),
-                              j ? u.y : u.x, ub, make_float2(j ? iu.y : iu.x, j ? iz.y : iz.x), exj, kc.lambda);
-            const float4 qc = make_float4(S.at(fQA, e, 0), S.at(fQA, e, 1), S.at(fQB, e, 0), S.at(fQB, e, 1));
-            const float4 qW = make_float4(S.at(fQA, e - 1, 0), 0.f, 0.f, S.at(fQB, e - 1, 1));
-            const float4 qN = make_float4(0.f, S.at(fQA, e - WX, 1), S.at(fQB, e - WX, 0), 0.f);
-            primal_px(cd, tau, mu, j ? make_float2(px.y, py.y) : make_float2(px.x, py.x), qc, qW, qN, un, ub, vb,
-                      make_float3(j ? ra.y : ra.x, j ? rb.y : rb.x, j ? rc.y : rc.x), make_float3(exj, eyj, ezj),
-                      kc.alpha0, kc.alpha1, &uo, &vo);
+        VFS_PAIR_NEIGHBOURS
+        float2 un, uo, vxo, vyo;
+        if (cl == 0) {
+          const float4 tc = S.tp(t);
+          float4 tw = S.tp(tW), tn = S.tp(tN);
+          if (seamW) tw.y = tw.x;
+          if (seamN) tn.w = tn.z;
+          const UV c = ld_uv(t);
+          const float2 tau2 = f2(tau);
+          const bool fast_tau = div_range(tau);
+          // l1Thresholding with all four neighbours unmasked (Python/vfs.cu:444-494)
+          const float2 gTx = psub(lo2(tc), lo2(tw)), gTy = psub(hi2(tc), hi2(tn));
+          const float4 ce = S.cE(t);
+          const float2 tauEtaU = fast_tau ? pdiv(tau2, lo2(ce), hi2(ce)) : make_float2(tau / -ce.x, tau / -ce.y);
+          const float2 uT = kFuseUT ? pfma(tauEtaU, padd(gTx, gTy), c.u) : padd(c.u, pmul(tauEtaU, padd(gTx, gTy)));
+          const float2 d = psub(uT, u);
+          const float2 rho = kFuseRho ? pfma(iu, d, iz) : padd(pmul(iu, d), iz);
+          const float2 t1 = pmul(f2(kc.lambda), tauEtaU);
+          const float2 t2 = pmul(t1, iu);
+          const float2 bound = pmul(t2, iu);
+          const float4 cu = S.cU(t);
+          float2 qr = pdiv(rho, lo2(cu), hi2(cu));
+          if (!(div_range(rho.x) && div_range(rho.y))) {
+            if (!div_range(rho.x)) qr.x = rho.x / iu.x;
+            if (!div_range(rho.y)) qr.y = rho.y / iu.y;
           }
-          if (j) u.y = un;
-          else u.x = un;
-          S.at(fUVA, e, 0) = uo;
-          S.at(fUVA, e, 1) = vo.x;
-          S.at(fUVB, e, 0) = vo.y;
+          const float2 dmid = psub(d, qr);
+          const float2 dlo = kFuseLo ? pfma(t1, iu, d) : padd(d, t2);
+          const float2 dhi = kFuseHi ? pfma(make_float2(-t1.x, -t1.y), iu, d) : psub(d, t2);
+          float2 du;
+          {
+            const float eps = 1E-7f;
+            const float mx = fabsf(iu.x) < eps ? d.x : dmid.x, my = fabsf(iu.y) < eps ? d.y : dmid.y;
+            du.x = (rho.x <= bound.x && rho.x >= -bound.x) ? mx
+                   : rho.x < -bound.x                      ? dlo.x
+                   : rho.x > bound.x                       ? dhi.x
+                                                           : 0.f;
+            du.y = (rho.y <= bound.y && rho.y >= -bound.y) ? my
+                   : rho.y < -bound.y                      ? dlo.y
+                   : rho.y > bound.y                       ? dhi.y
+                                                           : 0.f;
+          }
+          un = padd(u, du);
+          // keeps the primal step's loads below this point (fewer live registers)
+          asm volatile("" ::: "memory");
+          // updatePrimalVariables with all four neighbours unmasked (Python/vfs.cu:533-569)
+          const float4 qa = S.qA(t), qb = S.qB(t);
+          float4 qwa = S.qA(tW), qwb = S.qB(tW), qna = S.qA(tN), qnb = S.qB(tN);
+          if (seamW) qwa.y = qwa.x, qwb.w = qwb.z;
+          if (seamN) qna.w = qna.z, qnb.y = qnb.x;
+          const float2 gQx = psub(lo2(qa), lo2(qwa)), gQw = psub(hi2(qb), hi2(qwb));
+          const float2 gQy = psub(hi2(qa), hi2(qna)), gQz = psub(lo2(qb), lo2(qnb));
+          const float2 tux = pfma(ra, px, pmul(rc, py)), tuy = pfma(rc, px, pmul(rb, py));
+          const float4 cy = S.cY(t), cz = S.cZ(t);
+          const float2 te1 = fast_tau ? pdiv(tau2, lo2(cy), hi2(cy)) : make_float2(tau / -cy.x, tau / -cy.y);
+          const float2 te2 = fast_tau ? pdiv(tau2, lo2(cz), hi2(cz)) : make_float2(tau / -cz.x, tau / -cz.y);
+          const float2 Vx = pfma(te1, pfma(f2(kc.alpha1), tux, pmul(f2(kc.alpha0), padd(gQx, gQz))), c.vx);
+          const float2 Vy = pfma(te2, pfma(f2(kc.alpha1), tuy, pmul(f2(kc.alpha0), padd(gQw, gQy))), c.vy);
+          uo = pfma(f2(mu), psub(un, c.u), un);
+          vxo = pfma(f2(mu), psub(Vx, c.vx), Vx), vyo = pfma(f2(mu), psub(Vy, c.vy), Vy);
+        } else {
+          pair_primal_lanes<NT, WX>(S, t, info, ra, rb, rc, iu, iz, u, px, py, tau, mu, kc.lambda, kc.alpha0,
+                                    kc.alpha1, un, uo, vxo, vyo);
         }
+        u = un;
+        S.uvA(t) = make_float4(uo.x, uo.y, vxo.x, vxo.y);
+        S.uvB(t) = vyo;
       }
     }
     __syncthreads();
   }
+
+#undef VFS_PAIR_NEIGHBOURS
 
   // ---- write back the tile (real pixels only)
 #pragma unroll
@@ -461,16 +503,18 @@ __device__ __forceinline__ void tgv_pair_tile(const TgvState& in, const TgvState
     const int X = x0 + tx, Y = y0 + ty;
     if (X >= w || Y >= h) continue;
     const long f = (long)Y * w + X;
+    const float4 uvA = S.uvA(t), qA = S.qA(t), qB = S.qB(t);
+    const float2 uvB = S.uvB(t);
     out.u[f] = j ? u.y : u.x;
-    out.ub[f] = S.at(fUVA, e, 0);
-    out.vbx[f] = S.at(fUVA, e, 1);
-    out.vby[f] = S.at(fUVB, e, 0);
+    out.ub[f] = j ? uvA.y : uvA.x;
+    out.vbx[f] = j ? uvA.w : uvA.z;
+    out.vby[f] = j ? uvB.y : uvB.x;
     out.px[f] = j ? px.y : px.x;
     out.py[f] = j ? py.y : py.x;
-    out.qx[f] = S.at(fQA, e, 0);
-    out.qy[f] = S.at(fQA, e, 1);
-    out.qz[f] = S.at(fQB, e, 0);
-    out.qw[f] = S.at(fQB, e, 1);
+    out.qx[f] = j ? qA.y : qA.x;
+    out.qy[f] = j ? qA.w : qA.z;
+    out.qz[f] = j ? qB.y : qB.x;
+    out.qw[f] = j ? qB.w : qB.z;
   }
 }
 
