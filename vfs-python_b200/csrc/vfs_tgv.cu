@@ -197,7 +197,6 @@ cudaError_t launch_block(const TgvState& in, const TgvState& out, const TgvConst
 }  // namespace vfs
 
 #include "vfs_tgv_reg.cuh"
-#include "vfs_tgv_pair.cuh"
 
 namespace vfs {
 namespace {
@@ -218,19 +217,19 @@ cudaError_t prepare_reg() {
 }
 
 template <int K, int TX, int TY, int NT>
-cudaError_t prepare_pair() {
-  cudaError_t e = cudaFuncSetAttribute(k_tgv_pair<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)pair_smem_bytes<K, TX, TY>(NT));
+cudaError_t prepare_rcp() {
+  cudaError_t e = cudaFuncSetAttribute(k_tgv_rcp<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)RegGeom<K, TX, TY>::smem_bytes_rcp());
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_tgv_pair_batch<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)pair_smem_bytes<K, TX, TY>(NT));
+  return cudaFuncSetAttribute(k_tgv_rcp_batch<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)RegGeom<K, TX, TY>::smem_bytes_rcp());
 }
 
 template <int K, int TX, int TY, int NT>
-cudaError_t batch_pair(const TgvBatchItem* items, int n_items, int total_tiles, int parity, const float3* sched,
-                       int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
-  k_tgv_pair_batch<K, TX, TY, NT><<<total_tiles, NT, pair_smem_bytes<K, TX, TY>(NT), s>>>(items, n_items, parity,
-                                                                                          sched, it0, niter, kc);
+cudaError_t batch_rcp(const TgvBatchItem* items, int n_items, int total_tiles, int parity, const float3* sched,
+                      int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
+  k_tgv_rcp_batch<K, TX, TY, NT><<<total_tiles, NT, RegGeom<K, TX, TY>::smem_bytes_rcp(), s>>>(
+      items, n_items, parity, sched, it0, niter, kc);
   return cudaGetLastError();
 }
 
@@ -283,16 +282,17 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
 }
 
 template <int K, int TX, int TY, int NT>
-cudaError_t launch_pair(const TgvState& in, const TgvState& out, const TgvConsts& c, const float3* sched, int it0,
-                        int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
+cudaError_t launch_rcp(const TgvState& in, const TgvState& out, const TgvConsts& c, const float3* sched, int it0,
+                       int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
   dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);
-  PdlLaunch L(grid, NT, pair_smem_bytes<K, TX, TY>(NT), s);
-  return cudaLaunchKernelEx(&L.cfg, k_tgv_pair<K, TX, TY, NT>, in, out, c, sched, it0, niter, kc, h, w);
+  PdlLaunch L(grid, NT, RegGeom<K, TX, TY>::smem_bytes_rcp(), s);
+  return cudaLaunchKernelEx(&L.cfg, k_tgv_rcp<K, TX, TY, NT>, in, out, c, sched, it0, niter, kc, h, w);
 }
 
 // Compiled variants: id -> (implementation, iterations per launch, tile).
 // Ids below 100 keep all state in shared memory; ids 1xx are register-owned.
-// Ids 3xx are the two-pixel lockstep kernels (vfs_tgv_pair.cuh).
+// Ids 4xx are the reciprocal forms of the register-owned kernels of the same
+// shape (the last two digits), which divide through precomputed reciprocals.
 // Ids 22x have tiles sized so that a pyramid level of side S = 12 T covers
 // at most 144 tiles, one per SM of the 148: the 1024-thread kernels hold one
 // CTA per SM, so 169 tiles of a power-of-two side would need a second wave
@@ -348,12 +348,14 @@ cudaError_t launch_pair(const TgvState& in, const TgvState& out, const TgvConsts
   X(224, reg, 6, 9, 9, 736)          \
   X(225, reg, 4, 11, 11, 544)        \
   X(226, reg, 4, 27, 27, 1024)       \
-  X(320, pair, 3, 34, 34, 1024)      \
-  X(321, pair, 3, 36, 36, 1024)      \
-  X(334, pair, 4, 32, 32, 1024)      \
-  X(326, pair, 3, 22, 22, 512)       \
-  X(322, pair, 4, 17, 17, 448)       \
-  X(324, pair, 6, 8, 8, 352)
+  X(421, rcp, 3, 36, 36, 1024)       \
+  X(420, rcp, 3, 34, 34, 1024)       \
+  X(434, rcp, 4, 32, 32, 1024)       \
+  X(422, rcp, 4, 17, 17, 864)        \
+  X(423, rcp, 5, 17, 17, 1024)       \
+  X(413, rcp, 6, 8, 8, 704)          \
+  X(424, rcp, 6, 9, 9, 736)          \
+  X(407, rcp, 4, 8, 8, 416)
 
 // Register-owned variants also compiled in recording form (every
 // iteration's state written out), for the reverse mode's recomputation.

@@ -19,7 +19,7 @@ struct TgvState {
 // Per-warp constants, same flat layout: diffusion tensor (a, b, c), the
 // preconditioner eta (x, y, z), the image derivatives (iu, iz) and the mask
 // code (self/E/W/S/N bits).  rcp, where set, holds per pixel the
-// reciprocals the two-pixel kernels divide with (vfs_tgv_pair.cuh): those of
+// reciprocals the fused kernels divide with (vfs_tgv_reg.cuh): those of
 // eta.x, eta.y, eta.z (formed per level with the eta planes) and of iu
 // (formed per warp with the derivatives).
 struct TgvConsts {
