@@ -33,21 +33,6 @@ struct SolverConsts {
   const float2* dscale;
 };
 
-// ---------------------------------------------------------------- division helpers
-// of the fused TGV kernels (vfs_tgv_reg.cuh), which divide by a per-pixel
-// constant y through its reciprocal.  2^-60 <= |v| <= 2^60 (false for zeros,
-// subnormals, Inf and NaN): the range where the reciprocal method is exact.
-__device__ __forceinline__ bool div_range(float v) {
-  return (__float_as_uint(v) & 0x7fffffffu) - 0x21800000u <= 0x3C000000u;
-}
-// The eta a step divides by: below the reference's eps (1e-7) the reference
-// uses tau itself instead of tau / eta, and tau / 1 == tau.
-__device__ __forceinline__ float eta_used(float e) { return fabsf(e) < 1E-7f ? 1.f : e; }
-// RN(1 / y) in the range above, NaN outside it (the kernels then divide with '/').
-__device__ __forceinline__ float recip_or_nan(float y) {
-  return div_range(y) ? __frcp_rn(y) : __int_as_float(0x7fffffff);
-}
-
 // ---------------------------------------------------------------- K7 tensor
 // computeEta, Python/vfs.cu:228-237.
 __device__ __forceinline__ float3 compute_eta(float a, float b, float c, float a11, float a004) {
@@ -159,36 +144,6 @@ __device__ __forceinline__ float threshold_px(uint8_t code, float tau, float2 tp
 // ---------------------------------------------------------------- K12 primal
 // updatePrimalVariables_ for an unmasked pixel, Python/vfs.cu:533-569.
 // un: the thresholded u of this iteration; ub, vb: the previous bar iterates.
-// primal_q takes the two step quotients tauEta1 = tau / eta.y and tauEta2 =
-// tau / eta.z (each tau itself where |eta| < 1e-7) from the caller.
-__device__ __forceinline__ void primal_q(uint8_t code, float tauEta1, float tauEta2, float mu, float2 pc, float4 qc,
-                                         float4 qW, float4 qN, float un, float ub, float2 vb, float3 abc,
-                                         float alpha0, float alpha1, float* u_out, float2* v_out) {
-  float4 gradQ = make_float4(0, 0, 0, 0);
-  if (code & kE) {
-    gradQ.x = qc.x;
-    gradQ.w = qc.w;
-  }
-  if (code & kW) {
-    gradQ.x -= qW.x;
-    gradQ.w -= qW.w;
-  }
-  if (code & kS) {
-    gradQ.y = qc.y;
-    gradQ.z = qc.z;
-  }
-  if (code & kN) {
-    gradQ.y -= qN.y;
-    gradQ.z -= qN.z;
-  }
-  const float2 tu = make_float2(fmaf(abc.x, pc.x, abc.z * pc.y), fmaf(abc.z, pc.x, abc.y * pc.y));
-  const float2 updatedV = make_float2(fmaf(tauEta1, fmaf(alpha1, tu.x, alpha0 * (gradQ.x + gradQ.z)), vb.x),
-                                      fmaf(tauEta2, fmaf(alpha1, tu.y, alpha0 * (gradQ.w + gradQ.y)), vb.y));
-  *u_out = fmaf(mu, un - ub, un);
-  v_out->x = fmaf(mu, updatedV.x - vb.x, updatedV.x);
-  v_out->y = fmaf(mu, updatedV.y - vb.y, updatedV.y);
-}
-
 __device__ __forceinline__ void primal_px(uint8_t code, float tau, float mu, float2 pc, float4 qc, float4 qW,
                                           float4 qN, float un, float ub, float2 vb, float3 abc, float3 eta,
                                           float alpha0, float alpha1, float* u_out, float2* v_out) {
@@ -218,59 +173,6 @@ __device__ __forceinline__ void primal_px(uint8_t code, float tau, float mu, flo
   *u_out = fmaf(mu, un - ub, un);
   v_out->x = fmaf(mu, updatedV.x - vb.x, updatedV.x);
   v_out->y = fmaf(mu, updatedV.y - vb.y, updatedV.y);
-}
-
-// ---------------------------------------------------------------- reciprocal division
-// RN(x / y) from r = RN(1 / y), for x and y in the div_range: q0 = RN(x r) is
-// within 1.5 ulp of x / y, one correction q1 = RN(q0 + (x - y q0) r) brings it
-// within an ulp, and a second one gives the correctly rounded quotient, the
-// IEEE division's result (Markstein, "Computation of elementary functions on
-// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; the
-// remainders are exact FMAs).  Checked against '/' on a B200: no mismatch in
-// 67 M random quotients of the kernels' operand ranges and 0.64 M quotients
-// within 2^-48 of a rounding midpoint.
-__device__ __forceinline__ float div_rcp(float x, float y, float r) {
-  const float q0 = __fmul_rn(x, r);
-  const float q1 = __fmaf_rn(__fmaf_rn(-q0, y, x), r, q0);
-  return __fmaf_rn(__fmaf_rn(-q1, y, x), r, q1);
-}
-
-// The threshold step (l1Thresholding_, Python/vfs.cu:444-494) with its two
-// divisions through reciprocals: etaU is eta.x or 1 where |eta.x| < 1e-7
-// (then tau / 1 == tau), rx = RN(1 / etaU), riu = RN(1 / dIu); etaU, and dIu
-// where |dIu| >= 1e-7, are in the div_range (the caller checks), as is tau.
-// The multiply-adds are rounded as the reference kernel's are (the compiler
-// fuses uTauGtp and rho; the product lambda tauEtaU dIu is rounded on its
-// own, being shared with the bound), which a B200 comparison with
-// threshold_px over 4 M random pixels covering all three shrink cases pins.
-__device__ __forceinline__ float threshold_rcp(uint8_t code, float tau, float2 tpc, float2 tpW, float2 tpN, float u,
-                                               float ub, float2 deriv, float etaU, float rx, float riu,
-                                               float lambda) {
-  const float eps = 1E-7f;
-  float2 gradTp = make_float2(0, 0);
-  const bool e = code & kE, w = code & kW, s = code & kS, n = code & kN;
-  if (e && w) gradTp.x = __fsub_rn(tpc.x, tpW.x);
-  else if (!e) gradTp.x = -tpW.x;
-  else gradTp.x = tpc.x;
-  if (s && n) gradTp.y = __fsub_rn(tpc.y, tpN.y);
-  else if (!s) gradTp.y = -tpN.y;
-  else gradTp.y = tpc.y;
-  const float dIu = deriv.x, dIz = deriv.y;
-  const float tauEtaU = div_rcp(tau, etaU, rx);
-  const float uTauGtp = __fmaf_rn(tauEtaU, __fadd_rn(gradTp.x, gradTp.y), ub);
-  const float d = __fsub_rn(uTauGtp, u);
-  const float rho = __fmaf_rn(dIu, d, dIz);
-  const float t2 = __fmul_rn(__fmul_rn(lambda, tauEtaU), dIu);
-  const float bound = __fmul_rn(t2, dIu);
-  float du = 0.f;
-  if ((rho <= bound) && (rho >= -bound)) {
-    du = (fabsf(dIu) < eps) ? d : __fsub_rn(d, div_range(rho) ? div_rcp(rho, dIu, riu) : rho / dIu);
-  } else if (rho < -bound) {
-    du = __fadd_rn(d, t2);
-  } else if (rho > bound) {
-    du = __fsub_rn(d, t2);
-  }
-  return __fadd_rn(u, du);
 }
 
 }  // namespace vfs

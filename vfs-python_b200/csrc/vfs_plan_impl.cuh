@@ -28,7 +28,6 @@ struct VfsPlan {
   vfs::Plane<float2> tvec;
   vfs::TgvConsts cst;
   float* cplanes[8];
-  float4* rcp = nullptr;  // reciprocal records of the per-warp constants (TgvConsts::rcp)
   vfs::TgvState st[2];
   vfs::Plane<float> ubefore[2];
   vfs::Plane<float2> warp[2];

@@ -217,23 +217,6 @@ cudaError_t prepare_reg() {
 }
 
 template <int K, int TX, int TY, int NT>
-cudaError_t prepare_rcp() {
-  cudaError_t e = cudaFuncSetAttribute(k_tgv_rcp<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)RegGeom<K, TX, TY>::smem_bytes_rcp());
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_tgv_rcp_batch<K, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)RegGeom<K, TX, TY>::smem_bytes_rcp());
-}
-
-template <int K, int TX, int TY, int NT>
-cudaError_t batch_rcp(const TgvBatchItem* items, int n_items, int total_tiles, int parity, const float3* sched,
-                      int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
-  k_tgv_rcp_batch<K, TX, TY, NT><<<total_tiles, NT, RegGeom<K, TX, TY>::smem_bytes_rcp(), s>>>(
-      items, n_items, parity, sched, it0, niter, kc);
-  return cudaGetLastError();
-}
-
-template <int K, int TX, int TY, int NT>
 cudaError_t batch_reg(const TgvBatchItem* items, int n_items, int total_tiles, int parity, const float3* sched,
                       int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
   k_tgv_reg_batch<K, TX, TY, NT><<<total_tiles, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(items, n_items, parity,
@@ -281,18 +264,8 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
   return e;
 }
 
-template <int K, int TX, int TY, int NT>
-cudaError_t launch_rcp(const TgvState& in, const TgvState& out, const TgvConsts& c, const float3* sched, int it0,
-                       int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
-  dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);
-  PdlLaunch L(grid, NT, RegGeom<K, TX, TY>::smem_bytes_rcp(), s);
-  return cudaLaunchKernelEx(&L.cfg, k_tgv_rcp<K, TX, TY, NT>, in, out, c, sched, it0, niter, kc, h, w);
-}
-
 // Compiled variants: id -> (implementation, iterations per launch, tile).
 // Ids below 100 keep all state in shared memory; ids 1xx are register-owned.
-// Ids 4xx are the reciprocal forms of the register-owned kernels of the same
-// shape (the last two digits), which divide through precomputed reciprocals.
 // Ids 22x have tiles sized so that a pyramid level of side S = 12 T covers
 // at most 144 tiles, one per SM of the 148: the 1024-thread kernels hold one
 // CTA per SM, so 169 tiles of a power-of-two side would need a second wave
@@ -347,15 +320,7 @@ cudaError_t launch_rcp(const TgvState& in, const TgvState& out, const TgvConsts&
   X(223, reg, 5, 17, 17, 1024)       \
   X(224, reg, 6, 9, 9, 736)          \
   X(225, reg, 4, 11, 11, 544)        \
-  X(226, reg, 4, 27, 27, 1024)       \
-  X(421, rcp, 3, 36, 36, 1024)       \
-  X(420, rcp, 3, 34, 34, 1024)       \
-  X(434, rcp, 4, 32, 32, 1024)       \
-  X(422, rcp, 4, 17, 17, 864)        \
-  X(423, rcp, 5, 17, 17, 1024)       \
-  X(413, rcp, 6, 8, 8, 704)          \
-  X(424, rcp, 6, 9, 9, 736)          \
-  X(407, rcp, 4, 8, 8, 416)
+  X(226, reg, 4, 27, 27, 1024)
 
 // Register-owned variants also compiled in recording form (every
 // iteration's state written out), for the reverse mode's recomputation.
@@ -442,7 +407,7 @@ bool tgv_tile_shape(int variant, int* tx, int* ty) {
   case id:                                \
     *tx = TX;                             \
     *ty = TY;                             \
-    return std::string(#impl) != "block";
+    return std::string(#impl) == "reg";
     VFS_TGV_VARIANTS(VFS_SHAPE)
 #undef VFS_SHAPE
     default: return false;

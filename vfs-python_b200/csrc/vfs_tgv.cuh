@@ -18,14 +18,10 @@ struct TgvState {
 
 // Per-warp constants, same flat layout: diffusion tensor (a, b, c), the
 // preconditioner eta (x, y, z), the image derivatives (iu, iz) and the mask
-// code (self/E/W/S/N bits).  rcp, where set, holds per pixel the
-// reciprocals the fused kernels divide with (vfs_tgv_reg.cuh): those of
-// eta.x, eta.y, eta.z (formed per level with the eta planes) and of iu
-// (formed per warp with the derivatives).
+// code (self/E/W/S/N bits).
 struct TgvConsts {
   const float *a, *b, *c, *ex, *ey, *ez, *iu, *iz;
   const uint8_t* code;
-  const float4* rcp = nullptr;
 };
 
 // One image of a batched TGV launch: its two state sets (ping-pong), its

@@ -27,15 +27,7 @@ struct RegGeom {
   // the state (RegSmem: 40 bytes per window pixel packed, 36 as planes),
   // then (sigma, tau, mu, scaleP, scaleQ) of each of the launch's iterations
   static constexpr size_t smem_bytes() { return (size_t)N * (16 + 16 + 8) + 5 * K * sizeof(float); }
-  // the reciprocal form adds a 16-byte record per window pixel after the schedule
-  static constexpr size_t kRcpOffset = ((size_t)N * (16 + 16 + 8) + 5 * K * sizeof(float) + 15) / 16 * 16;
-  static constexpr size_t smem_bytes_rcp() { return kRcpOffset + (size_t)N * 16; }
 };
-
-// Mask-code bits the reciprocal form adds to a pixel's code: its divisors
-// are all in the div_range with their reciprocals formed (the reciprocal
-// divisions apply), and, from bit 8 up, the last phase the pixel takes part in.
-constexpr int kRcpOk = 32;
 
 // The shared-memory state of a tile, in one of two layouts with the same
 // values: PACKED keeps (u_, v_x, v_y, -) and q as float4 records and tp as a
@@ -77,12 +69,7 @@ struct RegSmem {
 // With TRACE, the state after iteration s (of this launch) is written to the
 // record s - 1 of the trace, whose planes are those of `out` moved by
 // (s - 1) * rec_stride floats, instead of the final state to `out`.
-//
-// With RCP (the reciprocal form) the kernel divides tau / eta and rho / dIu
-// through the per-pixel reciprocals of TgvConsts::rcp (div_rcp, exact), keeps
-// eta with the reference's eps folded in (1 where |eta| < 1e-7), and tests a
-// pixel's region membership with one comparison against its last phase.
-template <int K, int TX, int TY, int NT, bool TRACE = false, bool RCP = false>
+template <int K, int TX, int TY, int NT, bool TRACE = false>
 __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState& out, const TgvConsts& cst,
                                              const float3* __restrict__ sched, int it0, int niter,
                                              const SolverConsts& kc, int h, int w, int x0, int y0,
@@ -98,7 +85,6 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
 
   float ru[J], rpx[J], rpy[J], ra[J], rb[J], rc[J], rex[J], rey[J], rez[J], riu[J], riz[J];
   int rcode[J], rwx[J], rwy[J];
-  float4* const sRcp = reinterpret_cast<float4*>(reinterpret_cast<char*>(smem_raw) + G::kRcpOffset);
 
   // When launched as a programmatic dependent of the previous TGV launch this
   // CTA may start before that launch ends: the per-warp constants are read
@@ -128,27 +114,6 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     riu[j] = ok ? cst.iu[f] : 0.f;
     riz[j] = ok ? cst.iz[f] : 0.f;
     rcode[j] = ok ? cst.code[f] : 0;
-    if constexpr (RCP) {
-      // eta with the eps folded in, the reciprocal record in shared memory,
-      // the reciprocal-division flag and the last phase in the code
-      rex[j] = eta_used(rex[j]);
-      rey[j] = eta_used(rey[j]);
-      rez[j] = eta_used(rez[j]);
-      const float nan = __int_as_float(0x7fffffff);
-      const float4 r = ok && cst.rcp ? cst.rcp[f] : make_float4(nan, nan, nan, nan);
-      if (e < N) sRcp[e] = r;
-      const bool fd = div_range(rex[j]) && div_range(rey[j]) && div_range(rez[j]) && r.x == r.x && r.y == r.y &&
-                      r.z == r.z && (fabsf(riu[j]) < 1E-7f || (div_range(riu[j]) && r.w == r.w));
-      int last = 0;
-      for (int s = 1; s <= k; ++s) {
-        const int lo_d = 2 * K - 2 * (k - s) - 1;
-        const int hiX = 2 * K + TX + (k - s), hiY = 2 * K + TY + (k - s);
-        if (wx >= lo_d && wx < hiX && wy >= lo_d && wy < hiY) last = 2 * s - 1;
-        if (wx >= lo_d + 1 && wx < hiX && wy >= lo_d + 1 && wy < hiY) last = 2 * s;
-      }
-      if (e >= N) last = 0;
-      rcode[j] |= (fd ? kRcpOk : 0) | last << 8;
-    }
   }
   // a tile whose pixels are all masked ends with zero state (masked pixels
   // are written 0 every iteration): write that and skip the iterations
@@ -194,20 +159,15 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
   for (int s = 1; s <= k; ++s) {
     const float* const sc = sSch + 5 * (s - 1);
     const float3 ss = make_float3(sc[0], sc[1], sc[2]);  // (sigma, tau, mu)
-    const bool tau_ok = RCP && div_range(ss.y);           // tau in the reciprocal division's range
     const float scaleP = sc[3], scaleQ = sc[4];           // alpha1 sigma / etaP, alpha0 sigma / etaQ
     {  // dual step on [lo, hiX) x [lo, hiY)
       const int lo = 2 * K - 2 * (k - s) - 1;
       const int hiX = 2 * K + TX + (k - s), hiY = 2 * K + TY + (k - s);
 #pragma unroll
       for (int j = 0; j < J; ++j) {
-        if constexpr (RCP) {
-          if (2 * s - 1 > (rcode[j] >> 8)) continue;
-        } else {
-          if (rwx[j] < lo || rwx[j] >= hiX || rwy[j] < lo || rwy[j] >= hiY) continue;
-        }
+        if (rwx[j] < lo || rwx[j] >= hiX || rwy[j] < lo || rwy[j] >= hiY) continue;
         const int i = threadIdx.x + j * NT;
-        const uint8_t code = (uint8_t)(RCP ? rcode[j] & 31 : rcode[j]);
+        const uint8_t code = (uint8_t)rcode[j];
         if (!(code & kSelf)) {
           rpx[j] = rpy[j] = 0.f;
           S.set_tp(i, make_float2(0.f, 0.f));
@@ -232,13 +192,9 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
       const int hiX = 2 * K + TX + (k - s), hiY = 2 * K + TY + (k - s);
 #pragma unroll
       for (int j = 0; j < J; ++j) {
-        if constexpr (RCP) {
-          if (2 * s > (rcode[j] >> 8)) continue;
-        } else {
-          if (rwx[j] < lo || rwx[j] >= hiX || rwy[j] < lo || rwy[j] >= hiY) continue;
-        }
+        if (rwx[j] < lo || rwx[j] >= hiX || rwy[j] < lo || rwy[j] >= hiY) continue;
         const int i = threadIdx.x + j * NT;
-        const uint8_t code = (uint8_t)(RCP ? rcode[j] & 31 : rcode[j]);
+        const uint8_t code = (uint8_t)rcode[j];
         if (!(code & kSelf)) {
           ru[j] = 0.f;
           S.set_uv(i, make_float4(0.f, 0.f, 0.f, 0.f));
@@ -246,26 +202,15 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
         }
         const float4 c = S.uv(i);
         const float ub = c.x;
-        float un, uo;
+        const float un = threshold_px(code, ss.y, S.tp(i), make_float2(S.tp(i - 1).x, 0.f),
+                                      make_float2(0.f, S.tp(i - WX).y), ru[j], ub, make_float2(riu[j], riz[j]), rex[j],
+                                      kc.lambda);
+        float uo;
         float2 vo;
         const float4 qW = S.q(i - 1), qN = S.q(i - WX);
-        bool rdiv = false;
-        if constexpr (RCP) rdiv = (rcode[j] & kRcpOk) && tau_ok;
-        if (rdiv) {
-          const float4 r = sRcp[i];
-          un = threshold_rcp(code, ss.y, S.tp(i), make_float2(S.tp(i - 1).x, 0.f), make_float2(0.f, S.tp(i - WX).y),
-                             ru[j], ub, make_float2(riu[j], riz[j]), rex[j], r.x, r.w, kc.lambda);
-          primal_q(code, div_rcp(ss.y, rey[j], r.y), div_rcp(ss.y, rez[j], r.z), ss.z, make_float2(rpx[j], rpy[j]),
-                   S.q(i), make_float4(qW.x, 0.f, 0.f, qW.w), make_float4(0.f, qN.y, qN.z, 0.f), un, ub,
-                   make_float2(c.y, c.z), make_float3(ra[j], rb[j], rc[j]), kc.alpha0, kc.alpha1, &uo, &vo);
-        } else {
-          // (with RCP, eta holds the eps folded in: tau / 1 == tau, the same result)
-          un = threshold_px(code, ss.y, S.tp(i), make_float2(S.tp(i - 1).x, 0.f), make_float2(0.f, S.tp(i - WX).y),
-                            ru[j], ub, make_float2(riu[j], riz[j]), rex[j], kc.lambda);
-          primal_px(code, ss.y, ss.z, make_float2(rpx[j], rpy[j]), S.q(i), make_float4(qW.x, 0.f, 0.f, qW.w),
-                    make_float4(0.f, qN.y, qN.z, 0.f), un, ub, make_float2(c.y, c.z), make_float3(ra[j], rb[j], rc[j]),
-                    make_float3(rex[j], rey[j], rez[j]), kc.alpha0, kc.alpha1, &uo, &vo);
-        }
+        primal_px(code, ss.y, ss.z, make_float2(rpx[j], rpy[j]), S.q(i), make_float4(qW.x, 0.f, 0.f, qW.w),
+                  make_float4(0.f, qN.y, qN.z, 0.f), un, ub, make_float2(c.y, c.z), make_float3(ra[j], rb[j], rc[j]),
+                  make_float3(rex[j], rey[j], rez[j]), kc.alpha0, kc.alpha1, &uo, &vo);
         ru[j] = un;
         S.set_uv(i, make_float4(uo, vo.x, vo.y, 0.f));
       }
@@ -326,33 +271,6 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
     k_tgv_reg(TgvState in, TgvState out, TgvConsts cst, const float3* __restrict__ sched, int it0, int niter,
               SolverConsts kc, int h, int w) {
   tgv_reg_tile<K, TX, TY, NT>(in, out, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY);
-}
-
-// The reciprocal form (see tgv_reg_tile).
-template <int K, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
-    k_tgv_rcp(TgvState in, TgvState out, TgvConsts cst, const float3* __restrict__ sched, int it0, int niter,
-              SolverConsts kc, int h, int w) {
-  tgv_reg_tile<K, TX, TY, NT, false, true>(in, out, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX,
-                                           blockIdx.y * TY);
-}
-
-template <int K, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
-    k_tgv_rcp_batch(const TgvBatchItem* __restrict__ items, int n_items, int parity,
-                    const float3* __restrict__ sched, int it0, int niter, SolverConsts kc) {
-  int lo = 0, hi = n_items - 1;
-  const int bid = blockIdx.x;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (items[mid].tile_base <= bid) lo = mid;
-    else hi = mid - 1;
-  }
-  const TgvBatchItem& it = items[lo];
-  const int t = bid - it.tile_base;
-  const int ty = t / it.tiles_x, tx = t - ty * it.tiles_x;
-  tgv_reg_tile<K, TX, TY, NT, false, true>(it.st[parity], it.st[parity ^ 1], it.cst, sched, it0, niter, kc, it.h,
-                                           it.w, tx * TX, ty * TY);
 }
 
 // Recording: every iteration's state to the records 0..niter of the trace
