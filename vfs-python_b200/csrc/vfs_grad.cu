@@ -67,6 +67,15 @@ __device__ __forceinline__ T ld0(const T* a, long i, long n) {
   return (i >= 0 && i < n) ? a[i] : T(0);
 }
 
+// A cotangent contribution that is not finite is dropped.  The forward can
+// leave a few pixels with NaN state (beside an epipole, the epipolar
+// direction is undefined; the reference's kernels give the same NaNs); a
+// NaN state times a finite (even zero) cotangent is NaN, and the stencil
+// would carry it to every cotangent within a few iterations.  Such pixels
+// are treated as passing no gradient: every cotangent a reverse kernel
+// writes, and every scalar it accumulates, goes through fin0.
+__device__ __forceinline__ float fin0(float x) { return isfinite(x) ? x : 0.f; }
+
 // Sum of N per-thread values over the block (at most 1024 threads), added to
 // out[0..N).  Every thread of the block must call it.
 template <int N>
@@ -76,7 +85,7 @@ __device__ __forceinline__ void block_sum_to(const float (&v)[N], double* out) {
   const int lane = tid & 31, wid = tid >> 5;
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    float s = v[k];
+    float s = fin0(v[k]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) red[k][wid] = s;
@@ -336,8 +345,8 @@ __global__ void k_g_post(float2* __restrict__ gwarp, float* __restrict__ gu, flo
   const float delta = fminf(raw, limit);
   const float2 gw = gwarp[i];
   const float2 tv = tvec[i];
-  const float gd = gu[i] + gw.x * tv.x + gw.y * tv.y;
-  gtvec[i] = make_float2(delta * gw.x, delta * gw.y);
+  const float gd = fin0(gu[i] + gw.x * tv.x + gw.y * tv.y);
+  gtvec[i] = make_float2(fin0(delta * gw.x), fin0(delta * gw.y));
   if (raw < limit) {
     gu[i] -= gd;
     atomicAdd(guT + ix[12], gd);
@@ -436,16 +445,16 @@ __global__ void __launch_bounds__(kGX* kGY) k_rev1(RevArgs r) {
       gubl = -mu * gubn + gut;
       gvx = gVx - mu * gvbx;
       gvy = gVy - mu * gvby;
-      r.gc[3][i] += gex;
-      r.gc[4][i] += gey;
-      r.gc[5][i] += gez;
-      r.gc[6][i] += giu;
-      r.gc[7][i] += giz;
+      r.gc[3][i] += fin0(gex);
+      r.gc[4][i] += fin0(gey);
+      r.gc[5][i] += fin0(gez);
+      r.gc[6][i] += fin0(giu);
+      r.gc[7][i] += fin0(giz);
     }
-    r.g0.u[i] = gu;
-    r.g0.ub[i] = gubl;
-    r.g0.vbx[i] = gvx;
-    r.g0.vby[i] = gvy;
+    r.g0.u[i] = fin0(gu);
+    r.g0.ub[i] = fin0(gubl);
+    r.g0.vbx[i] = fin0(gvx);
+    r.g0.vby[i] = fin0(gvy);
     r.A[0][i] = Ax;
     r.A[1][i] = Ay;
     r.A[2][i] = Bv;
@@ -550,16 +559,16 @@ __global__ void __launch_bounds__(kGX* kGY) k_rev2(RevArgs r) {
       Cv[3] = scaleQ * gq1;
       Cv[4] = scaleQ * gq2;
       Cv[5] = scaleQ * gq3;
-      r.gc[0][i] += ga;
-      r.gc[1][i] += gb;
-      r.gc[2][i] += gcc;
+      r.gc[0][i] += fin0(ga);
+      r.gc[1][i] += fin0(gb);
+      r.gc[2][i] += fin0(gcc);
     }
-    r.g0.px[i] = gP0;
-    r.g0.py[i] = gP1;
-    r.g0.qx[i] = gQ[0];
-    r.g0.qy[i] = gQ[1];
-    r.g0.qz[i] = gQ[2];
-    r.g0.qw[i] = gQ[3];
+    r.g0.px[i] = fin0(gP0);
+    r.g0.py[i] = fin0(gP1);
+    r.g0.qx[i] = fin0(gQ[0]);
+    r.g0.qy[i] = fin0(gQ[1]);
+    r.g0.qz[i] = fin0(gQ[2]);
+    r.g0.qw[i] = fin0(gQ[3]);
 #pragma unroll
     for (int k = 0; k < 6; ++k) r.C[k][i] = Cv[k];
   }
@@ -603,9 +612,9 @@ __global__ void __launch_bounds__(kGX* kGY) k_rev3(RevArgs r) {
     gvx -= r.C[4][i + w];
     gvy -= r.C[3][i + w];
   }
-  r.g0.ub[i] = gub;
-  r.g0.vbx[i] = gvx;
-  r.g0.vby[i] = gvy;
+  r.g0.ub[i] = fin0(gub);
+  r.g0.vbx[i] = fin0(gvx);
+  r.g0.vby[i] = fin0(gvy);
 }
 
 // The three phases above in one kernel over a TX x TY tile.  The window is
@@ -784,11 +793,11 @@ __global__ void __launch_bounds__(NT) k_rev_tile(RevArgs r) {
       if (core) {
         const float inx = fmaf(al1, tpx, al0 * (gQx + gQz));
         const float iny = fmaf(al1, tpy, al0 * (gQw + gQy));
-        GC3[f] += sx ? 0.f : -te / ex * gte;
-        GC4[f] += sy ? 0.f : -t1 / ey * inx * gVx;
-        GC5[f] += sz ? 0.f : -t2 / ez * iny * gVy;
-        GC6[f] += giu;
-        GC7[f] += giz;
+        GC3[f] += fin0(sx ? 0.f : -te / ex * gte);
+        GC4[f] += fin0(sy ? 0.f : -t1 / ey * inx * gVx);
+        GC5[f] += fin0(sz ? 0.f : -t2 / ez * iny * gVy);
+        GC6[f] += fin0(giu);
+        GC7[f] += fin0(giz);
         acc[0] += gl;
         acc[1] += t1 * (gQx + gQz) * gVx + t2 * (gQw + gQy) * gVy;
         acc[2] += t1 * tpx * gVx + t2 * tpy * gVy;
@@ -798,7 +807,7 @@ __global__ void __launch_bounds__(NT) k_rev_tile(RevArgs r) {
     P(aY)[e] = Ay;
     P(aB)[e] = Bv;
     if (core) {
-      G0U[f] = gu;
+      G0U[f] = fin0(gu);
       P(lUB)[e] = gubl;
       P(lVX)[e] = gvx;
       P(lVY)[e] = gvy;
@@ -888,21 +897,21 @@ __global__ void __launch_bounds__(NT) k_rev_tile(RevArgs r) {
         ga += gUx * gtux;
         gb += gUy * gtuy;
         gcc += gUy * gtux + gUx * gtuy;
-        GC0[f] += ga;
-        GC1[f] += gb;
-        GC2[f] += gcc;
+        GC0[f] += fin0(ga);
+        GC1[f] += fin0(gb);
+        GC2[f] += fin0(gcc);
         acc[1] += sigma / r.k.etaQ * (gVxx * gq0 + gVyy * gq1 + gVz * gq2 + gVw * gq3);
         acc[2] += sigma / r.k.etaP * (tux * gP0 + tuy * gP1);
-        G0PX[f] = gP0;
-        G0PY[f] = gP1;
-        G0QX[f] = gq0;
-        G0QY[f] = gq1;
-        G0QZ[f] = gq2;
-        G0QW[f] = gq3;
+        G0PX[f] = fin0(gP0);
+        G0PY[f] = fin0(gP1);
+        G0QX[f] = fin0(gq0);
+        G0QY[f] = fin0(gq1);
+        G0QZ[f] = fin0(gq2);
+        G0QW[f] = fin0(gq3);
       }
     } else if (core) {
-      G0PX[f] = G0PY[f] = 0.f;
-      G0QX[f] = G0QY[f] = G0QZ[f] = G0QW[f] = 0.f;
+      G0PX[f] = fin0(G0PY[f] = 0.f);
+      G0QX[f] = fin0(G0QY[f] = G0QZ[f] = G0QW[f] = 0.f);
     }
 #pragma unroll
     for (int k = 0; k < 6; ++k) P(c0 + k)[e] = Cv[k];
@@ -946,9 +955,9 @@ __global__ void __launch_bounds__(NT) k_rev_tile(RevArgs r) {
       gvx -= P(c4)[e + WX];
       gvy -= P(c3)[e + WX];
     }
-    G0UB[f] = gub;
-    G0VX[f] = gvx;
-    G0VY[f] = gvy;
+    G0UB[f] = fin0(gub);
+    G0VX[f] = fin0(gvx);
+    G0VY[f] = fin0(gvy);
   }
   block_sum_to<3>(acc, r.scal + G_LAMBDA);
 }
@@ -1462,19 +1471,19 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     const int X = x0 + rx[j], Y = y0 + ry[j];
     if (X >= w || Y >= h) continue;
     const long f = (long)Y * w + X;
-    r.g_out.u[f] = gU[j];
-    r.g_out.ub[f] = gUB[j];
-    r.g_out.vbx[f] = gVX[j];
-    r.g_out.vby[f] = gVY[j];
-    r.g_out.px[f] = gPX[j];
-    r.g_out.py[f] = gPY[j];
-    r.g_out.qx[f] = gQ0[j];
-    r.g_out.qy[f] = gQ1[j];
-    r.g_out.qz[f] = gQ2[j];
-    r.g_out.qw[f] = gQ3[j];
+    r.g_out.u[f] = fin0(gU[j]);
+    r.g_out.ub[f] = fin0(gUB[j]);
+    r.g_out.vbx[f] = fin0(gVX[j]);
+    r.g_out.vby[f] = fin0(gVY[j]);
+    r.g_out.px[f] = fin0(gPX[j]);
+    r.g_out.py[f] = fin0(gPY[j]);
+    r.g_out.qx[f] = fin0(gQ0[j]);
+    r.g_out.qy[f] = fin0(gQ1[j]);
+    r.g_out.qz[f] = fin0(gQ2[j]);
+    r.g_out.qw[f] = fin0(gQ3[j]);
 #pragma unroll
     for (int q = 0; q < 8; ++q)
-      if (gca[q] != 0.f) r.gc[q][f] += gca[q];
+      if (gca[q] != 0.f) r.gc[q][f] += fin0(gca[q]);
   }
   block_sum_to<3>(acc, r.scal + G_LAMBDA);
 }
