@@ -574,6 +574,7 @@ def run_batched800(args, n, rank, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     barrier(n)
     tot = tgv = 0.0
+    tgv_level = None
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -583,13 +584,18 @@ def run_batched800(args, n, rank, local):
             e1.record()
             e1.synchronize()
             tot += e0.elapsed_time(e1) / 1e3
-            tgv += batch.stats()["tgv_ms"] / 1e3
+            st = batch.stats()
+            tgv += st["tgv_ms"] / 1e3
+            lv = st.get("tgv_ms_level")
+            if lv is not None:
+                tgv_level = list(lv) if tgv_level is None else [a + b for a, b in zip(tgv_level, lv)]
     barrier(n)
     t_max = max_over_ranks(tot, n)
     value = n * len(pairs) * args.steps / t_max
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (per-pair seeds)",
+            "tgv_ms_per_level_per_step": [x / args.steps for x in tgv_level] if tgv_level else None,
             "config": {"workload": f"batched 800x800: {len(pairs)} pairs per GPU, 5 levels x 10 warps x 100 TGV "
                                    "iterations, one batched graph + triangulate_flow per pair",
                        "pairs_per_gpu": len(pairs), "tgv_kernel_per_level": choice,
