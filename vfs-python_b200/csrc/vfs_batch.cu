@@ -4,12 +4,19 @@
 // workspace; all pairs share the solver parameters and so the number of
 // levels, warps and iterations.  The pairs advance through the coarse-to-fine
 // solve in lockstep: per level and warp, each pair's small per-warp kernels
-// run, then every TGV pass is ONE launch whose blocks cover the tiles of all
-// pairs (a (pair, tile) work list in device memory), so small coarse levels of
-// many pairs fill the GPU together.  The whole batch can be captured and
-// replayed as one CUDA graph.  No counterpart in the reference, whose solver
-// handles one pair per call (Python/vfs.py:460-533); per pair the results are
-// bit-identical to a single-pair solve.
+// run, then the TGV passes run over a (pair, tile) work list in device
+// memory.  The pairs of a level are cut into groups whose solver working set
+// (two state sets and the per-warp constants, 113 bytes a pixel) fits the
+// group budget (96 MiB by default, inside the 126 MB L2): a group's passes
+// are launched one after another, each launch covering all the group's
+// tiles, before the next group's.  Small coarse levels of many pairs so fill
+// the GPU together in one launch per pass, while a large fine level keeps
+// its state resident in L2 from pass to pass (one pair at 800x800 is ~72 MB;
+// eight pairs in one launch per pass would stream it from DRAM each pass).
+// The whole batch can be captured and replayed as one CUDA graph.  No
+// counterpart in the reference, whose solver handles one pair per call
+// (Python/vfs.py:460-533); per pair the results are bit-identical to a
+// single-pair solve, whatever the grouping.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -25,6 +32,13 @@ struct VfsBatch {
   std::vector<VfsPlan*> plans;
   TgvBatchItem* items = nullptr;  // device, L x n
   std::vector<int> total_tiles;   // per level
+  // per level: groups of consecutive pairs launched together (first pair,
+  // pair count, first tile, tile count)
+  struct Group {
+    int p0, np, bid0, ntiles;
+  };
+  std::vector<std::vector<Group>> groups;
+  size_t group_bytes = 96ull << 20;  // 0: all pairs of a level in one launch per pass
   int level_variant[32];
   bool use_graph = false;
   cudaStream_t gstream = nullptr;
@@ -95,6 +109,27 @@ int upload_items(VfsBatch* bt) {
     }
     bt->total_tiles[l] = base;
   }
+  // groups of consecutive pairs within the working-set budget
+  bt->groups.assign(bt->L, {});
+  for (int l = 0; l < bt->L; ++l) {
+    int i = 0;
+    while (i < bt->n) {
+      const TgvBatchItem& first = host[(size_t)l * bt->n + i];
+      VfsBatch::Group g{i, 0, first.tile_base, 0};
+      double bytes = 0;
+      while (i < bt->n) {
+        const TgvBatchItem& it = host[(size_t)l * bt->n + i];
+        const double b = 113.0 * it.h * it.w;
+        if (g.np > 0 && bt->group_bytes > 0 && bytes + b > (double)bt->group_bytes) break;
+        bytes += b;
+        ++g.np;
+        ++i;
+      }
+      const int end = i < bt->n ? host[(size_t)l * bt->n + i].tile_base : bt->total_tiles[l];
+      g.ntiles = end - g.bid0;
+      bt->groups[l].push_back(g);
+    }
+  }
   VFS_TRY_CUDA(cudaMemcpy(bt->items, host.data(), host.size() * sizeof(TgvBatchItem), cudaMemcpyHostToDevice),
                "work list upload");
   return VFS_OK;
@@ -124,18 +159,20 @@ int enqueue_batch(VfsBatch* bt, cudaStream_t s) {
         pair = bt->tev_used++;
         VFS_TRY_CUDA(cudaEventRecordWithFlags(bt->tev[2 * pair], s, ev_flags), "event record");
       }
-      for (int j = 0; j < npass; ++j) {
-        const int it0 = j * K;
-        VFS_TRY_CUDA(launch_tgv_batch(var, bt->items + (size_t)l * n, n, bt->total_tiles[l], j % 2,
-                                      bt->plans[0]->sched, it0, std::min(K, nIt - it0), bt->plans[0]->kc, s),
-                     "batched tgv");
+      for (const auto& g : bt->groups[l]) {
+        for (int j = 0; j < npass; ++j) {
+          const int it0 = j * K;
+          VFS_TRY_CUDA(launch_tgv_batch(var, bt->items + (size_t)l * n + g.p0, g.np, g.bid0, g.ntiles, j % 2,
+                                        bt->plans[0]->sched, it0, std::min(K, nIt - it0), bt->plans[0]->kc, s),
+                       "batched tgv");
+        }
+        nk += npass;
       }
-      nk += npass;
       if (pair >= 0) {
         VFS_TRY_CUDA(cudaEventRecordWithFlags(bt->tev[2 * pair + 1], s, ev_flags), "event record");
         bt->tev_level[pair] = l;
         bt->tev_bytes[pair] = 113.0 * px * nIt;
-        bt->tev_launches[pair] = npass;
+        bt->tev_launches[pair] = npass * (long long)bt->groups[l].size();
       }
       for (int i = 0; i < n; ++i) {
         ctx[i].npass = npass;  // the batched launches' parity decides the final state set
@@ -222,6 +259,14 @@ int vfs_batch_set_level_variant(VfsBatch* bt, int level, int variant) {
   if (!tgv_tile_shape(variant, &tx, &ty)) return fail(VFS_ERR_ARG, "batched solves need a 1xx kernel variant");
   if (bt->level_variant[level] == variant) return VFS_OK;
   bt->level_variant[level] = variant;
+  bt->drop_graph();
+  return upload_items(bt);
+}
+
+int vfs_batch_set_group_bytes(VfsBatch* bt, size_t bytes) {
+  if (!bt) return fail(VFS_ERR_ARG, "batch is NULL");
+  if (bt->group_bytes == bytes) return VFS_OK;
+  bt->group_bytes = bytes;
   bt->drop_graph();
   return upload_items(bt);
 }

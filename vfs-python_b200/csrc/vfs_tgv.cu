@@ -217,15 +217,15 @@ cudaError_t prepare_reg() {
 }
 
 template <int K, int TX, int TY, int NT>
-cudaError_t batch_reg(const TgvBatchItem* items, int n_items, int total_tiles, int parity, const float3* sched,
+cudaError_t batch_reg(const TgvBatchItem* items, int n_items, int bid0, int n_tiles, int parity, const float3* sched,
                       int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
-  k_tgv_reg_batch<K, TX, TY, NT><<<total_tiles, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(items, n_items, parity,
-                                                                                            sched, it0, niter, kc);
+  k_tgv_reg_batch<K, TX, TY, NT><<<n_tiles, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(items, n_items, bid0, parity,
+                                                                                        sched, it0, niter, kc);
   return cudaGetLastError();
 }
 
 template <int K, int TX, int TY, int NT>
-cudaError_t batch_block(const TgvBatchItem*, int, int, int, const float3*, int, int, const SolverConsts&,
+cudaError_t batch_block(const TgvBatchItem*, int, int, int, int, const float3*, int, int, const SolverConsts&,
                         cudaStream_t) {
   return cudaErrorInvalidValue;  // batched launches use the register-owned kernels
 }
@@ -414,13 +414,13 @@ bool tgv_tile_shape(int variant, int* tx, int* ty) {
   }
 }
 
-cudaError_t launch_tgv_batch(int variant, const TgvBatchItem* items, int n_items, int total_tiles, int parity,
+cudaError_t launch_tgv_batch(int variant, const TgvBatchItem* items, int n_items, int bid0, int n_tiles, int parity,
                              const float3* sched, int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
-  if (n_items <= 0 || total_tiles <= 0 || niter <= 0) return cudaSuccess;
+  if (n_items <= 0 || n_tiles <= 0 || niter <= 0) return cudaSuccess;
   if (!kc.dscale) return cudaErrorInvalidValue;  // dual-step scales not formed
   switch (variant) {
 #define VFS_BATCH_V(id, impl, K, TX, TY, NT) \
-  case id: return batch_##impl<K, TX, TY, NT>(items, n_items, total_tiles, parity, sched, it0, niter, kc, s);
+  case id: return batch_##impl<K, TX, TY, NT>(items, n_items, bid0, n_tiles, parity, sched, it0, niter, kc, s);
     VFS_TGV_VARIANTS(VFS_BATCH_V)
 #undef VFS_BATCH_V
     default: return cudaErrorInvalidValue;

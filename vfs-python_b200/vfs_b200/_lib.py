@@ -108,6 +108,7 @@ _SIGS = {
     "vfs_batch_triangulate_lsq": [_P, _I, _F, _F, _F, _P, _P, _P],
     "vfs_batch_set_level_variant": [_P, _I, _I],
     "vfs_batch_set_graph": [_P, _I],
+    "vfs_batch_set_group_bytes": [_P, _SZ],
     "vfs_batch_set_timing": [_P, _I],
     "vfs_batch_stats": [_P, ctypes.POINTER(VfsSolveStats)],
     "vfs_solve_stereo_static": [_PRM, _P, _SZ, _P, _P, _P, _P, _P, _P],

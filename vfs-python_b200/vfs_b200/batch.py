@@ -8,9 +8,10 @@ the reference, which solves one pair per ``VFS.solve_stereo`` call).
 
 All pairs share ``param``'s solver settings (``param.width/height`` are
 ignored).  Per pair the result is bit-identical to ``VFS.solve_stereo``; the
-pairs advance level by level together and each TGV pass is one kernel launch
-over the tiles of every pair, captured with the rest of the batch as one CUDA
-graph.
+pairs advance level by level together, and per level the pairs are cut into
+groups whose solver state fits a working-set budget (96 MiB by default, inside
+L2): each TGV pass of a group is one kernel launch over the group's tiles,
+captured with the rest of the batch as one CUDA graph.
 """
 from __future__ import annotations
 
@@ -59,9 +60,13 @@ class VFSBatch:
         for l, v in enumerate(choice):
             call("vfs_batch_set_level_variant", self._batch, l, int(v))
 
-    def configure(self, use_graph=None, timing=None):
+    def configure(self, use_graph=None, timing=None, group_bytes=None):
+        """group_bytes: working-set budget of a launch group (vfs_batch_set_group_bytes;
+        0: all pairs of a level in one launch per pass)."""
         if use_graph is not None:
             call("vfs_batch_set_graph", self._batch, 1 if use_graph else 0)
+        if group_bytes is not None:
+            call("vfs_batch_set_group_bytes", self._batch, int(group_bytes))
         if timing is not None:
             call("vfs_batch_set_timing", self._batch, 1 if timing else 0)
 
