@@ -219,7 +219,7 @@ VFS_API int vfs_batch_set_level_variant(VfsBatch* batch, int level, int variant)
 /* Working-set budget of a batched TGV launch group: per level, consecutive
  * pairs whose solver state (113 bytes a pixel) sums to at most `bytes` share
  * one launch per pass, and a group's passes all run before the next group's,
- * so a group's state stays in L2 between passes.  Default 96 MiB; 0 puts all
+ * so a group's state can stay in L2 between passes.  0 (the default) puts all
  * pairs of a level in one launch per pass.  Results do not depend on it. */
 VFS_API int vfs_batch_set_group_bytes(VfsBatch* batch, size_t bytes);
 VFS_API int vfs_batch_set_graph(VfsBatch* batch, int enable);

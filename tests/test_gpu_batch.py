@@ -52,14 +52,14 @@ def test_batched_solve_matches_single_pair_and_reference(gpu):
                 xb = batch.triangulate(i, cam, p.t, method=method).cpu().numpy()
                 xs = v.triangulate_flow(cam, p.t, method=method).cpu().numpy()
                 assert np.array_equal(_bits(xb), _bits(xs)), f"pair {i} xyz ({method})"
-    # the launch grouping changes the order of launches only: one group per
-    # level (all pairs in one launch per pass) and one pair per group agree
-    for gb in (0, 1):
+    # the launch grouping changes the order of launches only: one pair per
+    # group and groups of a budget agree with one group per level
+    for gb in (1, 96 << 20):
         batch.configure(group_bytes=gb)
         regrouped = [w.cpu().numpy() for w in batch.solve(refs, oths)]
         for i in range(len(pairs)):
             assert np.array_equal(_bits(regrouped[i]), _bits(warps[i])), f"pair {i} with group budget {gb}"
-    batch.configure(group_bytes=96 << 20)
+    batch.configure(group_bytes=0)
     # one pair against the reference's own kernels
     r = refpath.RefVFS(bench_params(*sizes[1], n_level=3, n_warp=2, n_iter=11), "bench")
     r.compute_pyramid_sizes()

@@ -4,16 +4,16 @@
 // workspace; all pairs share the solver parameters and so the number of
 // levels, warps and iterations.  The pairs advance through the coarse-to-fine
 // solve in lockstep: per level and warp, each pair's small per-warp kernels
-// run, then the TGV passes run over a (pair, tile) work list in device
-// memory.  The pairs of a level are cut into groups whose solver working set
-// (two state sets and the per-warp constants, 113 bytes a pixel) fits the
-// group budget (96 MiB by default, inside the 126 MB L2): a group's passes
-// are launched one after another, each launch covering all the group's
-// tiles, before the next group's.  Small coarse levels of many pairs so fill
-// the GPU together in one launch per pass, while a large fine level keeps
-// its state resident in L2 from pass to pass (one pair at 800x800 is ~72 MB;
-// eight pairs in one launch per pass would stream it from DRAM each pass).
-// The whole batch can be captured and replayed as one CUDA graph.  No
+// run, then each TGV pass is one launch whose blocks cover the tiles of all
+// pairs (a (pair, tile) work list in device memory), so small coarse levels
+// of many pairs fill the GPU together.  Optionally (vfs_batch_set_group_bytes)
+// the pairs of a level are cut into groups whose solver working set (two
+// state sets and the per-warp constants, 113 bytes a pixel) fits a budget:
+// a group's passes then all run before the next group's, each launch
+// covering the group's tiles.  (On a B200, one 800x800 pair per group did
+// not bring an 8-pair batch's finest level back to the single-pair time, so
+// the default is one group.)  The whole batch can be captured and replayed
+// as one CUDA graph.  No
 // counterpart in the reference, whose solver handles one pair per call
 // (Python/vfs.py:460-533); per pair the results are bit-identical to a
 // single-pair solve, whatever the grouping.
@@ -38,7 +38,7 @@ struct VfsBatch {
     int p0, np, bid0, ntiles;
   };
   std::vector<std::vector<Group>> groups;
-  size_t group_bytes = 96ull << 20;  // 0: all pairs of a level in one launch per pass
+  size_t group_bytes = 0;  // 0: all pairs of a level in one launch per pass
   int level_variant[32];
   bool use_graph = false;
   cudaStream_t gstream = nullptr;

@@ -218,11 +218,7 @@ cudaError_t prepare_reg() {
 
 template <int K, int TX, int TY, int NT>
 cudaError_t batch_reg(const TgvBatchItem* items, int n_items, int bid0, int n_tiles, int parity, const float3* sched,
-                      int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
-  k_tgv_reg_batch<K, TX, TY, NT><<<n_tiles, NT, RegGeom<K, TX, TY>::smem_bytes(), s>>>(items, n_items, bid0, parity,
-                                                                                        sched, it0, niter, kc);
-  return cudaGetLastError();
-}
+                      int it0, int niter, const SolverConsts& kc, cudaStream_t s);
 
 template <int K, int TX, int TY, int NT>
 cudaError_t batch_block(const TgvBatchItem*, int, int, int, int, const float3*, int, int, const SolverConsts&,
@@ -262,6 +258,16 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
             a.maxThreadsPerBlock, a.localSizeBytes);
   }
   return e;
+}
+
+// Batched launches are programmatic dependents of the previous launch too
+// (the work list is read before griddepcontrol.wait, the state after it).
+template <int K, int TX, int TY, int NT>
+cudaError_t batch_reg(const TgvBatchItem* items, int n_items, int bid0, int n_tiles, int parity, const float3* sched,
+                      int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
+  PdlLaunch L(dim3(n_tiles), NT, RegGeom<K, TX, TY>::smem_bytes(), s);
+  return cudaLaunchKernelEx(&L.cfg, k_tgv_reg_batch<K, TX, TY, NT>, items, n_items, bid0, parity, sched, it0, niter,
+                            kc);
 }
 
 // Compiled variants: id -> (implementation, iterations per launch, tile).

@@ -8,10 +8,10 @@ the reference, which solves one pair per ``VFS.solve_stereo`` call).
 
 All pairs share ``param``'s solver settings (``param.width/height`` are
 ignored).  Per pair the result is bit-identical to ``VFS.solve_stereo``; the
-pairs advance level by level together, and per level the pairs are cut into
-groups whose solver state fits a working-set budget (96 MiB by default, inside
-L2): each TGV pass of a group is one kernel launch over the group's tiles,
-captured with the rest of the batch as one CUDA graph.
+pairs advance level by level together and each TGV pass is one kernel launch
+over the tiles of every pair (or, with ``configure(group_bytes=...)``, of each
+group of pairs whose solver state fits that budget), captured with the rest of
+the batch as one CUDA graph.
 """
 from __future__ import annotations
 
