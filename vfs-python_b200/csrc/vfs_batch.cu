@@ -5,8 +5,9 @@
 // levels, warps and iterations.  The pairs advance through the coarse-to-fine
 // solve in lockstep: per level and warp, each pair's small per-warp kernels
 // run, then each TGV pass is one launch whose blocks cover the tiles of all
-// pairs (a (pair, tile) work list in device memory), so small coarse levels
-// of many pairs fill the GPU together.  Optionally (vfs_batch_set_group_bytes)
+// pairs (a (pair, tile) work list of up to 32 pairs, passed as the launch's
+// parameter; larger batches take one launch per 32 pairs), so small coarse
+// levels of many pairs fill the GPU together.  Optionally (vfs_batch_set_group_bytes)
 // the pairs of a level are cut into groups whose solver working set (two
 // state sets and the per-warp constants, 113 bytes a pixel) fits a budget:
 // a group's passes then all run before the next group's, each launch
@@ -30,7 +31,7 @@ struct VfsBatch {
   VfsParams prm;
   int n = 0, L = 0;
   std::vector<VfsPlan*> plans;
-  TgvBatchItem* items = nullptr;  // device, L x n
+  std::vector<TgvBatchItem> items;  // L x n, passed to the launches as parameters
   std::vector<int> total_tiles;   // per level
   // per level: groups of consecutive pairs launched together (first pair,
   // pair count, first tile, tile count)
@@ -73,7 +74,7 @@ int layout_sizes(const VfsParams* prm, int n, const int* hs, const int* ws, std:
   std::string why;
   if (!valid_params(prm, &why)) return fail(VFS_ERR_ARG, why);
   if (n <= 0 || !hs || !ws) return fail(VFS_ERR_ARG, "a batch needs n > 0 pairs and their sizes");
-  size_t off = rup((size_t)prm->nLevel * n * sizeof(TgvBatchItem), kBatchAlign);
+  size_t off = 0;
   offs->clear();
   for (int i = 0; i < n; ++i) {
     VfsParams p = pair_params(prm, hs[i], ws[i]);
@@ -86,9 +87,10 @@ int layout_sizes(const VfsParams* prm, int n, const int* hs, const int* ws, std:
   return VFS_OK;
 }
 
-// Uploads the (pair, tile) work lists of every level for the chosen kernels.
+// The (pair, tile) work lists of every level for the chosen kernels.
 int upload_items(VfsBatch* bt) {
-  std::vector<TgvBatchItem> host((size_t)bt->L * bt->n);
+  std::vector<TgvBatchItem>& host = bt->items;
+  host.assign((size_t)bt->L * bt->n, TgvBatchItem{});
   bt->total_tiles.assign(bt->L, 0);
   for (int l = 0; l < bt->L; ++l) {
     int tx = 32, ty = 32;
@@ -121,6 +123,7 @@ int upload_items(VfsBatch* bt) {
         const TgvBatchItem& it = host[(size_t)l * bt->n + i];
         const double b = 113.0 * it.h * it.w;
         if (g.np > 0 && bt->group_bytes > 0 && bytes + b > (double)bt->group_bytes) break;
+        if (g.np == kBatchParamItems) break;  // a launch's work list holds at most this many
         bytes += b;
         ++g.np;
         ++i;
@@ -130,8 +133,6 @@ int upload_items(VfsBatch* bt) {
       bt->groups[l].push_back(g);
     }
   }
-  VFS_TRY_CUDA(cudaMemcpy(bt->items, host.data(), host.size() * sizeof(TgvBatchItem), cudaMemcpyHostToDevice),
-               "work list upload");
   return VFS_OK;
 }
 
@@ -160,10 +161,14 @@ int enqueue_batch(VfsBatch* bt, cudaStream_t s) {
         VFS_TRY_CUDA(cudaEventRecordWithFlags(bt->tev[2 * pair], s, ev_flags), "event record");
       }
       for (const auto& g : bt->groups[l]) {
+        TgvBatchParams P;
+        P.n_items = g.np;
+        P.bid0 = g.bid0;
+        for (int i = 0; i < g.np; ++i) P.items[i] = bt->items[(size_t)l * n + g.p0 + i];
         for (int j = 0; j < npass; ++j) {
           const int it0 = j * K;
-          VFS_TRY_CUDA(launch_tgv_batch(var, bt->items + (size_t)l * n + g.p0, g.np, g.bid0, g.ntiles, j % 2,
-                                        bt->plans[0]->sched, it0, std::min(K, nIt - it0), bt->plans[0]->kc, s),
+          VFS_TRY_CUDA(launch_tgv_batch(var, P, g.ntiles, j % 2, bt->plans[0]->sched, it0, std::min(K, nIt - it0),
+                                        bt->plans[0]->kc, s),
                        "batched tgv");
         }
         nk += npass;
@@ -224,7 +229,6 @@ int vfs_batch_create(const VfsParams* prm, int n, const int* heights, const int*
   bt->n = n;
   bt->L = prm->nLevel;
   for (int l = 0; l < 32; ++l) bt->level_variant[l] = 134;
-  bt->items = reinterpret_cast<TgvBatchItem*>(base);
   for (int i = 0; i < n; ++i) {
     VfsParams p = pair_params(prm, heights[i], widths[i]);
     VfsPlan* pl = nullptr;

@@ -217,12 +217,11 @@ cudaError_t prepare_reg() {
 }
 
 template <int K, int TX, int TY, int NT>
-cudaError_t batch_reg(const TgvBatchItem* items, int n_items, int bid0, int n_tiles, int parity, const float3* sched,
-                      int it0, int niter, const SolverConsts& kc, cudaStream_t s);
+cudaError_t batch_reg(const TgvBatchParams& P, int n_tiles, int parity, const float3* sched, int it0, int niter,
+                      const SolverConsts& kc, cudaStream_t s);
 
 template <int K, int TX, int TY, int NT>
-cudaError_t batch_block(const TgvBatchItem*, int, int, int, int, const float3*, int, int, const SolverConsts&,
-                        cudaStream_t) {
+cudaError_t batch_block(const TgvBatchParams&, int, int, const float3*, int, int, const SolverConsts&, cudaStream_t) {
   return cudaErrorInvalidValue;  // batched launches use the register-owned kernels
 }
 
@@ -263,11 +262,10 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
 // Batched launches are programmatic dependents of the previous launch too
 // (the work list is read before griddepcontrol.wait, the state after it).
 template <int K, int TX, int TY, int NT>
-cudaError_t batch_reg(const TgvBatchItem* items, int n_items, int bid0, int n_tiles, int parity, const float3* sched,
-                      int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
+cudaError_t batch_reg(const TgvBatchParams& P, int n_tiles, int parity, const float3* sched, int it0, int niter,
+                      const SolverConsts& kc, cudaStream_t s) {
   PdlLaunch L(dim3(n_tiles), NT, RegGeom<K, TX, TY>::smem_bytes(), s);
-  return cudaLaunchKernelEx(&L.cfg, k_tgv_reg_batch<K, TX, TY, NT>, items, n_items, bid0, parity, sched, it0, niter,
-                            kc);
+  return cudaLaunchKernelEx(&L.cfg, k_tgv_reg_batch<K, TX, TY, NT>, P, parity, sched, it0, niter, kc);
 }
 
 // Compiled variants: id -> (implementation, iterations per launch, tile).
@@ -420,13 +418,14 @@ bool tgv_tile_shape(int variant, int* tx, int* ty) {
   }
 }
 
-cudaError_t launch_tgv_batch(int variant, const TgvBatchItem* items, int n_items, int bid0, int n_tiles, int parity,
-                             const float3* sched, int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
-  if (n_items <= 0 || n_tiles <= 0 || niter <= 0) return cudaSuccess;
+cudaError_t launch_tgv_batch(int variant, const TgvBatchParams& P, int n_tiles, int parity, const float3* sched,
+                             int it0, int niter, const SolverConsts& kc, cudaStream_t s) {
+  if (P.n_items <= 0 || n_tiles <= 0 || niter <= 0) return cudaSuccess;
+  if (P.n_items > kBatchParamItems) return cudaErrorInvalidValue;
   if (!kc.dscale) return cudaErrorInvalidValue;  // dual-step scales not formed
   switch (variant) {
 #define VFS_BATCH_V(id, impl, K, TX, TY, NT) \
-  case id: return batch_##impl<K, TX, TY, NT>(items, n_items, bid0, n_tiles, parity, sched, it0, niter, kc, s);
+  case id: return batch_##impl<K, TX, TY, NT>(P, n_tiles, parity, sched, it0, niter, kc, s);
     VFS_TGV_VARIANTS(VFS_BATCH_V)
 #undef VFS_BATCH_V
     default: return cudaErrorInvalidValue;

@@ -35,12 +35,21 @@ struct TgvBatchItem {
 // Tile shape of a register-owned variant (false for other variants).
 bool tgv_tile_shape(int variant, int* tx, int* ty);
 
-// Batched launch of a register-owned variant over n_tiles blocks, the tiles
-// bid0 .. bid0 + n_tiles - 1 of the items' tile numbering (TgvBatchItem::
-// tile_base): the items (in device memory) read st[parity] and write
-// st[parity ^ 1].
-cudaError_t launch_tgv_batch(int variant, const TgvBatchItem* items, int n_items, int bid0, int n_tiles, int parity,
-                             const float3* sched, int it0, int niter, const SolverConsts& kc, cudaStream_t s);
+// The work list of one batched launch, passed by value as the kernel's
+// parameter (so the kernel reads the items' pointers from the constant
+// parameter space, as a single-image launch reads its arguments): up to
+// kBatchParamItems images whose tiles are bid0 .. bid0 + n_tiles - 1 of the
+// items' tile numbering (TgvBatchItem::tile_base).
+constexpr int kBatchParamItems = 32;
+struct TgvBatchParams {
+  int n_items, bid0;
+  TgvBatchItem items[kBatchParamItems];
+};
+
+// Batched launch of a register-owned variant over n_tiles blocks: the items
+// read st[parity] and write st[parity ^ 1].
+cudaError_t launch_tgv_batch(int variant, const TgvBatchParams& P, int n_tiles, int parity, const float3* sched,
+                             int it0, int niter, const SolverConsts& kc, cudaStream_t s);
 
 // Sets the kernels' shared-memory attributes (call before any graph capture).
 cudaError_t tgv_prepare();

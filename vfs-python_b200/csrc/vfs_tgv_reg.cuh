@@ -284,22 +284,22 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
 }
 
 // Batched: one launch over the tiles of many images (the pairs of a batch at
-// the same pyramid level and pass).  items[i].tile_base is the first block of
-// item i counted from bid0 (the launch covers blocks bid0 .. bid0 + grid - 1
-// of the items' numbering); block b belongs to the last item whose
+// the same pyramid level and pass).  P.items[i].tile_base is the first block
+// of item i in the items' numbering, of which the launch covers blocks
+// P.bid0 .. P.bid0 + grid - 1; block b belongs to the last item whose
 // tile_base <= b.
 template <int K, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
-    k_tgv_reg_batch(const TgvBatchItem* __restrict__ items, int n_items, int bid0, int parity,
-                    const float3* __restrict__ sched, int it0, int niter, SolverConsts kc) {
-  int lo = 0, hi = n_items - 1;
-  const int bid = bid0 + (int)blockIdx.x;
+    k_tgv_reg_batch(const __grid_constant__ TgvBatchParams P, int parity, const float3* __restrict__ sched, int it0,
+                    int niter, SolverConsts kc) {
+  int lo = 0, hi = P.n_items - 1;
+  const int bid = P.bid0 + (int)blockIdx.x;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (items[mid].tile_base <= bid) lo = mid;
+    if (P.items[mid].tile_base <= bid) lo = mid;
     else hi = mid - 1;
   }
-  const TgvBatchItem& it = items[lo];
+  const TgvBatchItem& it = P.items[lo];
   const int t = bid - it.tile_base;
   const int ty = t / it.tiles_x, tx = t - ty * it.tiles_x;
   tgv_reg_tile<K, TX, TY, NT>(it.st[parity], it.st[parity ^ 1], it.cst, sched, it0, niter, kc, it.h, it.w, tx * TX,
