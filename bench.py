@@ -17,7 +17,9 @@ the timed events).  ``e2e``: the same through the public Python API from
 pinned host images, with the host->device copy of both images and the
 device->host copy of the depth map inside the timed region.  ``batched``: the
 32-pair uneven workload in one batched graph (pairs sharded over ranks by
-cost).  ``parity_vs_reference``: after the timed region, the same pair solved
+cost); ``batched800``: eight pairs of the headline configuration per GPU in
+one batched graph (the fused-batched form of ``value``, which solves one pair
+at a time).  ``parity_vs_reference``: after the timed region, the same pair solved
 by the reference's own kernels (oracle/_ref), compared bit for bit.
 
 With N > 1 GPUs (``--gpus N`` starts the N ranks through torch.distributed.run
@@ -465,6 +467,8 @@ def run_b200(args, n, rank, local):
     del flush
     if not args.no_batched:
         line["batched"] = run_batched(args, n, rank, local, steps=max(3, min(args.steps, 10)))
+        # the same 800x800 configuration fused-batched: 8 pairs per GPU in one batched graph
+        line["batched800"] = run_batched800(args, n, rank, local, steps=max(3, min(args.steps, 5)))
     if rank == 0 and not args.no_parity:
         line["parity_vs_reference"] = parity_vs_reference(pair, p, flow_np, xyz_np)
     if n == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -540,13 +544,14 @@ def run_batched(args, n, rank, local, steps=None):
             "tgv_share_of_step": tgv / tot if tot else None, "clocks": clk.summary()}
 
 
-def run_batched800(args, n, rank, local):
+def run_batched800(args, n, rank, local, steps=None):
     """The 800x800 drop-in configuration (5 levels x 10 warps x 100
     iterations) for several pairs at once (per-pair seeds): one batched graph
     per step, then each pair's triangulation.  Batching fills the SMs on the
     latency-bound coarse levels, which one pair alone cannot."""
     import multiprocessing as mpc
     from vfs_b200.batch import VFSBatch
+    steps = steps or args.steps
     from vfs_b200 import EquidistantCam
     from vfs_b200.synthetic import vector_fields
     seeds = [rank * args.pairs + i for i in range(args.pairs)]
@@ -576,7 +581,7 @@ def run_batched800(args, n, rank, local):
     tot = tgv = 0.0
     tgv_level = None
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
@@ -591,11 +596,11 @@ def run_batched800(args, n, rank, local):
                 tgv_level = list(lv) if tgv_level is None else [a + b for a, b in zip(tgv_level, lv)]
     barrier(n)
     t_max = max_over_ranks(tot, n)
-    value = n * len(pairs) * args.steps / t_max
-    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+    value = n * len(pairs) * steps / t_max
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (per-pair seeds)",
-            "tgv_ms_per_level_per_step": [x / args.steps for x in tgv_level] if tgv_level else None,
+            "tgv_ms_per_level_per_step": [x / steps for x in tgv_level] if tgv_level else None,
             "config": {"workload": f"batched 800x800: {len(pairs)} pairs per GPU, 5 levels x 10 warps x 100 TGV "
                                    "iterations, one batched graph + triangulate_flow per pair",
                        "pairs_per_gpu": len(pairs), "tgv_kernel_per_level": choice,
