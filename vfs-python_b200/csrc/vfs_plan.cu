@@ -54,6 +54,11 @@ __global__ void k_tensor_soa(TgvConsts out, uint8_t* code, cudaTextureObject_t s
   const_cast<float*>(out.ex)[i] = e.x;
   const_cast<float*>(out.ey)[i] = e.y;
   const_cast<float*>(out.ez)[i] = e.z;
+  if (out.rec) {
+    float4* r = const_cast<float4*>(out.rec) + 2 * i;
+    r[0] = make_float4(a.x, a.y, a.z, e.x);
+    *reinterpret_cast<float2*>(r + 1) = make_float2(e.y, e.z);
+  }
 }
 
 // computeDerivatives (Python/vfs.cu:304-324) plus the per-warp solver reset
@@ -68,6 +73,7 @@ __global__ void k_derivs_init(TgvConsts out, TgvState st, Plane<const float> ube
   const float2 d = epipolar_derivs(tref, tother, tdir, X, Y, h, w);
   const_cast<float*>(out.iu)[i] = d.x;
   const_cast<float*>(out.iz)[i] = d.y;
+  if (out.rec) reinterpret_cast<float2*>(const_cast<float4*>(out.rec) + 2 * i + 1)[1] = d;
   const float ubv = ub_src.at(X, Y);
   st.u[i] = ubefore.at(X, Y);
   st.ub[i] = ubv;
@@ -128,6 +134,7 @@ size_t layout(VfsPlan* pl, char* base) {
   pl->warped = {cv.take<float>(pitch_of(w0, 4) * h0), pitch_of(w0, 4)};
   pl->tvec = {cv.take<float2>(n0 * 8), 0};
   for (int i = 0; i < 8; ++i) pl->cplanes[i] = cv.take<float>(n0 * 4);
+  pl->crec = cv.take<float4>(n0 * 32);
   for (int b = 0; b < 2; ++b) {
     float** f[10] = {&pl->st[b].u, &pl->st[b].ub, &pl->st[b].vbx, &pl->st[b].vby, &pl->st[b].px,
                      &pl->st[b].py, &pl->st[b].qx, &pl->st[b].qy, &pl->st[b].qz, &pl->st[b].qw};
@@ -140,7 +147,7 @@ size_t layout(VfsPlan* pl, char* base) {
   pl->stage_ref = cv.take<uint8_t>(n0);
   pl->stage_other = cv.take<uint8_t>(n0);
   pl->cst = {pl->cplanes[0], pl->cplanes[1], pl->cplanes[2], pl->cplanes[3], pl->cplanes[4],
-             pl->cplanes[5], pl->cplanes[6], pl->cplanes[7], nullptr};
+             pl->cplanes[5], pl->cplanes[6], pl->cplanes[7], nullptr, pl->crec};
   return cv.off + kAlign;
 }
 

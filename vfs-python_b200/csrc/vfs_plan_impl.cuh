@@ -28,6 +28,7 @@ struct VfsPlan {
   vfs::Plane<float2> tvec;
   vfs::TgvConsts cst;
   float* cplanes[8];
+  float4* crec = nullptr;  // the constants as records (TgvConsts::rec)
   vfs::TgvState st[2];
   vfs::Plane<float> ubefore[2];
   vfs::Plane<float2> warp[2];

@@ -246,6 +246,7 @@ struct PdlLaunch {
 template <int K, int TX, int TY, int NT>
 cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts& c, const float3* sched, int it0,
                        int niter, const SolverConsts& kc, int h, int w, cudaStream_t s) {
+  if (!c.rec) return cudaErrorInvalidValue;
   dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY);
   PdlLaunch L(grid, NT, RegGeom<K, TX, TY>::smem_bytes(), s);
   cudaError_t e = cudaLaunchKernelEx(&L.cfg, k_tgv_reg<K, TX, TY, NT>, in, out, c, sched, it0, niter, kc, h, w);
@@ -264,6 +265,8 @@ cudaError_t launch_reg(const TgvState& in, const TgvState& out, const TgvConsts&
 template <int K, int TX, int TY, int NT>
 cudaError_t batch_reg(const TgvBatchParams& P, int n_tiles, int parity, const float3* sched, int it0, int niter,
                       const SolverConsts& kc, cudaStream_t s) {
+  for (int i = 0; i < P.n_items; ++i)
+    if (!P.items[i].cst.rec) return cudaErrorInvalidValue;
   PdlLaunch L(dim3(n_tiles), NT, RegGeom<K, TX, TY>::smem_bytes(), s);
   return cudaLaunchKernelEx(&L.cfg, k_tgv_reg_batch<K, TX, TY, NT>, P, parity, sched, it0, niter, kc);
 }
@@ -370,7 +373,7 @@ cudaError_t launch_tgv_trace(int variant, const TgvState& in, const TgvState& tr
                              const TgvConsts& c, const float3* sched, int it0, int niter, const SolverConsts& kc,
                              int h, int w, cudaStream_t s) {
   if (h <= 0 || w <= 0 || niter <= 0) return cudaSuccess;
-  if (!kc.dscale) return cudaErrorInvalidValue;  // dual-step scales not formed
+  if (!kc.dscale || !c.rec) return cudaErrorInvalidValue;  // dual-step scales or constant records missing
   switch (variant) {
 #define VFS_LAUNCH_T(id, K, TX, TY, NT)                                                                    \
   case id: {                                                                                               \

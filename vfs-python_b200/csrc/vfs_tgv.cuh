@@ -22,6 +22,11 @@ struct TgvState {
 struct TgvConsts {
   const float *a, *b, *c, *ex, *ey, *ez, *iu, *iz;
   const uint8_t* code;
+  // the same constants as two 16-byte records per pixel, rec[2 f] =
+  // (a, b, c, ex) and rec[2 f + 1] = (ey, ez, iu, iz): the register-owned
+  // kernels load them with two vector loads instead of eight scalar ones
+  // (required by those kernels; the others read the planes)
+  const float4* rec = nullptr;
 };
 
 // One image of a batched TGV launch: its two state sets (ping-pong), its

@@ -105,14 +105,10 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     rwy[j] = e < N ? wy : 1 << 20;  // never inside a region
     const long f = base + (long)wy * w + wx;
     const bool ok = e < N && f >= 0 && f < n;
-    ra[j] = ok ? cst.a[f] : 0.f;
-    rb[j] = ok ? cst.b[f] : 0.f;
-    rc[j] = ok ? cst.c[f] : 0.f;
-    rex[j] = ok ? cst.ex[f] : 0.f;
-    rey[j] = ok ? cst.ey[f] : 0.f;
-    rez[j] = ok ? cst.ez[f] : 0.f;
-    riu[j] = ok ? cst.iu[f] : 0.f;
-    riz[j] = ok ? cst.iz[f] : 0.f;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 r0 = ok ? cst.rec[2 * f] : z, r1 = ok ? cst.rec[2 * f + 1] : z;
+    ra[j] = r0.x, rb[j] = r0.y, rc[j] = r0.z, rex[j] = r0.w;
+    rey[j] = r1.x, rez[j] = r1.y, riu[j] = r1.z, riz[j] = r1.w;
     rcode[j] = ok ? cst.code[f] : 0;
   }
   // a tile whose pixels are all masked ends with zero state (masked pixels
