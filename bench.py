@@ -457,7 +457,7 @@ def run_b200(args, n, rank, local):
         plain_ms = 1e3 * t_max / args.steps
         fbs = {}
         for ck in (10, 1):
-            fb = fwd_bwd_timing(pair, p, ckpt=ck, plain_ms=plain_ms, flush=flush)
+            fb = fwd_bwd_timing(pair, p, ckpt=ck, plain_ms=plain_ms, flush=flush, local=local)
             fb["ms_fwd_bwd"] = max_over_ranks(fb["ms_fwd_bwd"], n)
             fb["ratio_to_forward"] = fb["ms_fwd_bwd"] / plain_ms
             fb["fwd_bwd_per_s"] = n * 1e3 / fb["ms_fwd_bwd"]
@@ -708,7 +708,7 @@ def reverse_roofline(solver, run_once):
             "traffic": (tr["dram_bytes_per_alg_byte"] * st["tgv_alg_bytes"] / max(st["tgv_launches"], 1)) if tr else None}
 
 
-def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None):
+def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None, local=0):
     """Forward + hand-written backward of one solve through DepthSolver (L1
     depth loss against the pair's ground truth), per-level reverse forms
     autotuned first.  Device time with inputs resident."""
@@ -726,22 +726,23 @@ def fwd_bwd_timing(pair, p, steps=3, warmup=1, ckpt=1, plain_ms=None, flush=None
         _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid)
     torch.cuda.synchronize()
     f_ms = b_ms = 0.0
-    for _ in range(steps):
-        if flush is not None:
-            flush.zero_()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        e[0].record()
-        depth = solver.forward_pass(ref_f, oth_f, t, theta)
-        e[1].record()
-        m = loss_mask(depth, valid)
-        g = torch.where(m, torch.sign(depth - gt), torch.zeros_like(depth)) / m.sum().clamp(min=1)
-        solver.backward_pass(g)
-        e[2].record()
-        torch.cuda.synchronize()
-        f_ms += e[0].elapsed_time(e[1])
-        b_ms += e[1].elapsed_time(e[2])
+    with ClockSampler(local) as clk:
+        for _ in range(steps):
+            if flush is not None:
+                flush.zero_()
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record()
+            depth = solver.forward_pass(ref_f, oth_f, t, theta)
+            e[1].record()
+            m = loss_mask(depth, valid)
+            g = torch.where(m, torch.sign(depth - gt), torch.zeros_like(depth)) / m.sum().clamp(min=1)
+            solver.backward_pass(g)
+            e[2].record()
+            torch.cuda.synchronize()
+            f_ms += e[0].elapsed_time(e[1])
+            b_ms += e[1].elapsed_time(e[2])
     out = {"ms_fwd_bwd": (f_ms + b_ms) / steps, "ms_recording_forward": f_ms / steps, "ms_backward": b_ms / steps,
-           "ckpt_every": ckpt, "reverse_forms_per_level": forms,
+           "clocks": clk.summary(), "ckpt_every": ckpt, "reverse_forms_per_level": forms,
            "recording_forward_variants": getattr(solver, "level_variants", None),
            "workspace_gb": solver.workspace_bytes / 1e9,
            "roofline": reverse_roofline(solver, lambda: _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid))}

@@ -288,7 +288,7 @@ VFS_API int vfs_grad_forward(VfsGradPlan* plan, const float* img_ref, const floa
 VFS_API int vfs_grad_backward(VfsGradPlan* plan, const float* g_depth, float* g_ref, float* g_other,
                               double* g_scalars, void* stream);
 /* Backward kernels: fused_reverse selects how an iteration is reversed:
- * 11..20 (default 11) several iterations per launch, cotangent state on chip
+ * 11..20 (default 11) two to four iterations per launch, cotangent state on chip
  * (11: 2 iterations, 24x16 tiles; 12: 2, 16x16; 13: 3, 16x16; 14: 4, 16x8;
  * 15: 2, 8x8; 16: 4, 8x8; 17: 3, 24x12; 18: 2, 32x12; 19: 3, 20x15;
  * 20: 2, 28x16), 1..5 one iteration per launch in one tiled kernel

@@ -1181,6 +1181,17 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     if (e < N && rx[j] >= -1 && rx[j] <= TX && ry[j] >= -1 && ry[j] <= TY && (scode[e] & kSelf)) live = 1;
   }
   live = __syncthreads_or(live);
+  // a warp whose pixels and their four neighbours are all unmasked with
+  // all four neighbours unmasked (most of the image) takes the phases
+  // compiled for that code: no code tests, no neighbour-code loads (not
+  // for tiles below 16x16, which measured faster without it)
+  bool wfull = false;
+  if constexpr (TX * TY >= 256) {
+    const int e = threadIdx.x;
+    const bool ring = e >= WX && e + WX < N && scode[e] == kAllSides && scode[e - 1] == kAllSides &&
+                      scode[e + 1] == kAllSides && scode[e - WX] == kAllSides && scode[e + WX] == kAllSides;
+    wfull = __all_sync(0xffffffffu, ring);
+  }
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
   if (!live) {
 #pragma unroll
@@ -1229,8 +1240,8 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       if (rx[j] < lo - 1 || rx[j] >= hiX + 2 || ry[j] < lo - 1 || ry[j] >= hiY + 2) continue;
       const int e = threadIdx.x + j * NT;
       const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LHX);
-      const uint8_t c = scode[e];
       const bool core = rx[j] >= 0 && rx[j] < TX && ry[j] >= 0 && ry[j] < TY && x0 + rx[j] < w && y0 + ry[j] < h;
+      auto phase1 = [&](const uint8_t c) {
       float Ax = 0.f, Ay = 0.f, Bv = 0.f;
       if (f >= 0 && f < n && (c & kSelf)) {
         const float gubn = gUB[j], gvbx = gVX[j], gvby = gVY[j];
@@ -1304,6 +1315,9 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       P(bAX)[e] = Ax;
       P(bAY)[e] = Ay;
       P(bAB)[e] = Bv;
+      };
+      if (wfull) phase1(kAllSides);
+      else phase1(scode[e]);
     }
     __syncthreads();
     // phase 2: dual step reversed on [lo - 1, hi + 1)
@@ -1314,11 +1328,11 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       if (rx[j] < lo - 1 || rx[j] >= hiX + 1 || ry[j] < lo - 1 || ry[j] >= hiY + 1) continue;
       const int e = threadIdx.x + j * NT;
       const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LHX);
-      const uint8_t c = scode[e];
       const bool core = rx[j] >= 0 && rx[j] < TX && ry[j] >= 0 && ry[j] < TY && x0 + rx[j] < w && y0 + ry[j] < h;
+      auto phase2 = [&](const uint8_t c, const bool full) {
       float Cv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       if (f >= 0 && f < n && (c & kSelf)) {
-        const uint8_t cE = scode[e + 1], cS = scode[e + WX];
+        const uint8_t cE = full ? kAllSides : scode[e + 1], cS = full ? kAllSides : scode[e + WX];
         const float Bv = P(bAB)[e];
         const float gVx = (1.f + mu) * gVX[j], gVy = (1.f + mu) * gVY[j];
         const float rey = P(bREY)[e], rez = P(bREZ)[e];
@@ -1407,6 +1421,9 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
       }
 #pragma unroll
       for (int q = 0; q < 6; ++q) P(bC0 + q)[e] = Cv[q];
+      };
+      if (wfull) phase2(kAllSides, true);
+      else phase2(scode[e], false);
     }
     // phase 3 and the next step's phase 1 share one barrier interval: the
     // state that phase 1 reads first (loaded a step ahead) is waited for here
@@ -1422,8 +1439,8 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     for (int j = 0; j < J; ++j) {
       if (rx[j] < lo || rx[j] >= hiX || ry[j] < lo || ry[j] >= hiY) continue;
       const int e = threadIdx.x + j * NT;
-      const uint8_t c = scode[e];
       float gub = lUB[j], gvx = lVX[j], gvy = lVY[j];
+      auto phase3 = [&](const uint8_t c, const uint8_t cW, const uint8_t cE, const uint8_t cN, const uint8_t cS) {
       if (c & kSelf) {
         const float u0 = P(bC0)[e], u1 = P(bC0 + 1)[e];
         const float v0 = P(bC0 + 2)[e], v1 = P(bC0 + 3)[e], v2 = P(bC0 + 4)[e], v3 = P(bC0 + 5)[e];
@@ -1431,26 +1448,29 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
         gvx += -u0 + ((c & kE) ? -v0 : v0) + ((c & kS) ? -v2 : v2);
         gvy += -u1 + ((c & kE) ? -v3 : v3) + ((c & kS) ? -v1 : v1);
       }
-      if (scode[e - 1] & kE) {
+      if (cW & kE) {
         gub += P(bC0)[e - 1];
         gvx += P(bC0 + 2)[e - 1];
         gvy += P(bC0 + 5)[e - 1];
       }
-      if (!(scode[e + 1] & kE)) {
+      if (!(cE & kE)) {
         gub -= P(bC0)[e + 1];
         gvx -= P(bC0 + 2)[e + 1];
         gvy -= P(bC0 + 5)[e + 1];
       }
-      if (scode[e - WX] & kS) {
+      if (cN & kS) {
         gub += P(bC0 + 1)[e - WX];
         gvx += P(bC0 + 4)[e - WX];
         gvy += P(bC0 + 3)[e - WX];
       }
-      if (!(scode[e + WX] & kS)) {
+      if (!(cS & kS)) {
         gub -= P(bC0 + 1)[e + WX];
         gvx -= P(bC0 + 4)[e + WX];
         gvy -= P(bC0 + 3)[e + WX];
       }
+      };
+      if (wfull) phase3(kAllSides, kAllSides, kAllSides, kAllSides, kAllSides);
+      else phase3(scode[e], scode[e - 1], scode[e + 1], scode[e - WX], scode[e + WX]);
       gU[j] = nU[j];
       gUB[j] = gub;
       gVX[j] = gvx;
@@ -1493,6 +1513,11 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 // with 140 tiles, one wave on the 148 SMs, where 17 needs 153; 20 is the
 // widest tile whose window (36x23) fits one pixel per thread within the
 // register budget, recomputing 1.85 window pixels per tile pixel (11: 1.92).
+// One iteration per launch with wider tiles (28x20, 32x18, 24x24 at 864-896
+// threads: 1.54 window pixels per tile pixel) measured 1.5x slower at
+// 800x800 than these forms: the constants, cotangents and states are then
+// loaded and the cotangents of the constants written back once per
+// iteration.
 #define VFS_REVB_SHAPES(X) \
   X(11, 2, 24, 16, 736)    \
   X(12, 2, 16, 16, 576)    \

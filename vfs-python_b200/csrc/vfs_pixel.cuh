@@ -17,6 +17,8 @@ namespace vfs {
 // texture at X+-1 / Y+-1, which returns the edge texel outside the image;
 // Python/vfs.cu:345, 359, 371, 448-467, 537-553).
 enum : uint8_t { kSelf = 1, kE = 2, kW = 4, kS = 8, kN = 16 };
+// the code of an unmasked pixel whose four neighbours are unmasked
+constexpr uint8_t kAllSides = kSelf | kE | kW | kS | kN;
 
 // Run-time solver constants.  The reference bakes these into the source text
 // (Python/vfs.py:57-68); the float members hold the values as the reference's

@@ -19,6 +19,9 @@
 namespace vfs {
 namespace {
 
+// the flag added to the codes of a warp whose pixels all have kAllSides
+constexpr uint8_t kWarpFull = 32;
+
 template <int K, int TX, int TY>
 struct RegGeom {
   static constexpr int WX = TX + 3 * K;
@@ -76,6 +79,9 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
                                              long rec_stride = 0) {
   using G = RegGeom<K, TX, TY>;
   constexpr int WX = G::WX, N = G::N, J = (N + NT - 1) / NT;
+  // the fast path for fully unmasked warps; the small tiles of the coarse
+  // levels (mostly halo and mask edge) measured faster without it
+  constexpr bool kFast = TX * TY >= 256;
   extern __shared__ float4 smem_raw[];
   const RegSmem<J == 1, N> S{smem_raw};
   float* const sSch = reinterpret_cast<float*>(smem_raw) + 10 * N;  // after 40 N bytes
@@ -110,6 +116,10 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     ra[j] = r0.x, rb[j] = r0.y, rc[j] = r0.z, rex[j] = r0.w;
     rey[j] = r1.x, rez[j] = r1.y, riu[j] = r1.z, riz[j] = r1.w;
     rcode[j] = ok ? cst.code[f] : 0;
+    // warps whose pixels are all unmasked with all four neighbours unmasked
+    // (most of the image) take a path compiled for that code
+    if constexpr (kFast)
+      if (__all_sync(0xffffffffu, rcode[j] == kAllSides)) rcode[j] |= kWarpFull;
   }
   // a tile whose pixels are all masked ends with zero state (masked pixels
   // are written 0 every iteration): write that and skip the iterations
@@ -164,22 +174,33 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
         if (rwx[j] < lo || rwx[j] >= hiX || rwy[j] < lo || rwy[j] >= hiY) continue;
         const int i = threadIdx.x + j * NT;
         const uint8_t code = (uint8_t)rcode[j];
-        if (!(code & kSelf)) {
+        // the unmasked step; with the code the literal kAllSides (full) the
+        // compiler drops the code tests and the W/N loads, which only
+        // pixels without an E/S neighbour read
+        auto step = [&](uint8_t cd, bool full) {
+          float2 p = make_float2(rpx[j], rpy[j]), tp;
+          float4 q = S.q(i);
+          const float4 c = S.uv(i), cE = S.uv(i + 1), cS = S.uv(i + WX);
+          // (with the fast path compiled in, the other kernels skip them
+          // by the code's bits too: fewer registers there)
+          const float4 cW = (full || (kFast && (cd & kE))) ? c : S.uv(i - 1);
+          const float4 cN = (full || (kFast && (cd & kS))) ? c : S.uv(i - WX);
+          dual_px(cd, c.x, make_float2(c.y, c.z), cE.x, make_float2(cE.y, cE.z), cW.x, make_float2(cW.y, cW.z), cS.x,
+                  make_float2(cS.y, cS.z), cN.x, make_float2(cN.y, cN.z), make_float3(ra[j], rb[j], rc[j]), scaleP,
+                  scaleQ, &p, &tp, &q);
+          rpx[j] = p.x;
+          rpy[j] = p.y;
+          S.set_tp(i, tp);
+          S.set_q(i, q);
+        };
+        auto masked = [&] {
           rpx[j] = rpy[j] = 0.f;
           S.set_tp(i, make_float2(0.f, 0.f));
           S.set_q(i, make_float4(0.f, 0.f, 0.f, 0.f));
-          continue;
-        }
-        float2 p = make_float2(rpx[j], rpy[j]), tp;
-        float4 q = S.q(i);
-        const float4 c = S.uv(i), cE = S.uv(i + 1), cW = S.uv(i - 1), cS = S.uv(i + WX), cN = S.uv(i - WX);
-        dual_px(code, c.x, make_float2(c.y, c.z), cE.x, make_float2(cE.y, cE.z), cW.x, make_float2(cW.y, cW.z),
-                cS.x, make_float2(cS.y, cS.z), cN.x, make_float2(cN.y, cN.z), make_float3(ra[j], rb[j], rc[j]), scaleP,
-                scaleQ, &p, &tp, &q);
-        rpx[j] = p.x;
-        rpy[j] = p.y;
-        S.set_tp(i, tp);
-        S.set_q(i, q);
+        };
+        if (kFast && (code & kWarpFull)) step(kAllSides, true);
+        else if (!(code & kSelf)) masked();
+        else step(code, false);
       }
     }
     __syncthreads();
@@ -191,24 +212,28 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
         if (rwx[j] < lo || rwx[j] >= hiX || rwy[j] < lo || rwy[j] >= hiY) continue;
         const int i = threadIdx.x + j * NT;
         const uint8_t code = (uint8_t)rcode[j];
-        if (!(code & kSelf)) {
+        auto step = [&](uint8_t cd) {
+          const float4 c = S.uv(i);
+          const float ub = c.x;
+          const float un = threshold_px(cd, ss.y, S.tp(i), make_float2(S.tp(i - 1).x, 0.f),
+                                        make_float2(0.f, S.tp(i - WX).y), ru[j], ub, make_float2(riu[j], riz[j]),
+                                        rex[j], kc.lambda);
+          float uo;
+          float2 vo;
+          const float4 qW = S.q(i - 1), qN = S.q(i - WX);
+          primal_px(cd, ss.y, ss.z, make_float2(rpx[j], rpy[j]), S.q(i), make_float4(qW.x, 0.f, 0.f, qW.w),
+                    make_float4(0.f, qN.y, qN.z, 0.f), un, ub, make_float2(c.y, c.z), make_float3(ra[j], rb[j], rc[j]),
+                    make_float3(rex[j], rey[j], rez[j]), kc.alpha0, kc.alpha1, &uo, &vo);
+          ru[j] = un;
+          S.set_uv(i, make_float4(uo, vo.x, vo.y, 0.f));
+        };
+        auto masked = [&] {
           ru[j] = 0.f;
           S.set_uv(i, make_float4(0.f, 0.f, 0.f, 0.f));
-          continue;
-        }
-        const float4 c = S.uv(i);
-        const float ub = c.x;
-        const float un = threshold_px(code, ss.y, S.tp(i), make_float2(S.tp(i - 1).x, 0.f),
-                                      make_float2(0.f, S.tp(i - WX).y), ru[j], ub, make_float2(riu[j], riz[j]), rex[j],
-                                      kc.lambda);
-        float uo;
-        float2 vo;
-        const float4 qW = S.q(i - 1), qN = S.q(i - WX);
-        primal_px(code, ss.y, ss.z, make_float2(rpx[j], rpy[j]), S.q(i), make_float4(qW.x, 0.f, 0.f, qW.w),
-                  make_float4(0.f, qN.y, qN.z, 0.f), un, ub, make_float2(c.y, c.z), make_float3(ra[j], rb[j], rc[j]),
-                  make_float3(rex[j], rey[j], rez[j]), kc.alpha0, kc.alpha1, &uo, &vo);
-        ru[j] = un;
-        S.set_uv(i, make_float4(uo, vo.x, vo.y, 0.f));
+        };
+        if (kFast && (code & kWarpFull)) step(kAllSides);
+        else if (!(code & kSelf)) masked();
+        else step(code);
       }
     }
     if constexpr (TRACE) {  // each thread writes the tile pixels it owns

@@ -75,7 +75,7 @@ class DepthSolver:
 
     def set_options(self, fused_reverse: int = 11, trace_variant: int = 0) -> None:
         """Backward kernel forms (see vfs_grad_set_options in vfs_b200.h): the
-        reverse-step kernel (11..20 several iterations per launch, 1..5 one
+        reverse-step kernel (11..20 two to four iterations per launch, 1..5 one
         tiled kernel per iteration, 0 three gather kernels) and the TGV variant
         recomputing checkpoint intervals (0 automatic, -1 one iteration per launch)."""
         call("vfs_grad_set_options", self._gp, int(fused_reverse), int(trace_variant))
