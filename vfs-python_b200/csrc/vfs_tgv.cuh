@@ -8,6 +8,21 @@
 
 namespace vfs {
 
+// Asynchronous global -> shared copies (cp.async): 4 or 16 bytes, zero-filled
+// where !ok (the source is then not read); a commit closes a group, a wait
+// blocks until at most NG groups are still in flight.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async16(float* dst, const float* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NG>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NG) : "memory"); }
+
 // Solver state of one warp, structure of arrays, flat row-major planes of
 // h*w floats (row stride exactly w, as the reference's flat neighbour reads
 // assume).  u: thresholded flow increment; ub, vbx, vby: the over-relaxed

@@ -50,6 +50,15 @@ struct RegSmem {
     if constexpr (PACKED) base[i] = v;
     else pl(0)[i] = v.x, pl(1)[i] = v.y, pl(2)[i] = v.z;
   }
+  // addresses of component c of pixel i's (u_, v_x, v_y) and q values
+  __device__ __forceinline__ float* uv_at(int i, int c) const {
+    if constexpr (PACKED) return reinterpret_cast<float*>(base + i) + c;
+    else return pl(c) + i;
+  }
+  __device__ __forceinline__ float* q_at(int i, int c) const {
+    if constexpr (PACKED) return reinterpret_cast<float*>(base + N + i) + c;
+    else return pl(3 + c) + i;
+  }
   __device__ __forceinline__ float4 q(int i) const {
     if constexpr (PACKED) return base[N + i];
     else return make_float4(pl(3)[i], pl(4)[i], pl(5)[i], pl(6)[i]);
@@ -155,10 +164,28 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
     ru[j] = ok ? in.u[f] : 0.f;
     rpx[j] = ok ? in.px[f] : 0.f;
     rpy[j] = ok ? in.py[f] : 0.f;
-    if (e < N) {
+    if (e >= N) continue;
+    if constexpr (J > 1) {
+      // planes: the shared-memory state straight from global memory with
+      // cp.async (zero-filled outside the image), no register staging
+      // (800^2 and 400^2 levels 2-3 % faster)
+      const long g = ok ? f : 0;
+      cp_async4(S.uv_at(e, 0), in.ub + g, ok);
+      cp_async4(S.uv_at(e, 1), in.vbx + g, ok);
+      cp_async4(S.uv_at(e, 2), in.vby + g, ok);
+      cp_async4(S.q_at(e, 0), in.qx + g, ok);
+      cp_async4(S.q_at(e, 1), in.qy + g, ok);
+      cp_async4(S.q_at(e, 2), in.qz + g, ok);
+      cp_async4(S.q_at(e, 3), in.qw + g, ok);
+    } else {
+      // records: one 16-byte store each (faster here than seven 4-byte copies)
       S.set_uv(e, ok ? make_float4(in.ub[f], in.vbx[f], in.vby[f], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f));
       S.set_q(e, ok ? make_float4(in.qx[f], in.qy[f], in.qz[f], in.qw[f]) : make_float4(0.f, 0.f, 0.f, 0.f));
     }
+  }
+  if constexpr (J > 1) {
+    cp_async_commit();
+    cp_async_wait<0>();
   }
   __syncthreads();
 
