@@ -704,7 +704,7 @@ def reverse_roofline(solver, run_once):
             "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": kind,
             "alg_bytes_per_pixel_iteration": 241, "alg_bytes_per_launch": st["tgv_alg_bytes"] / max(st["tgv_launches"], 1),
             "avg_launch_us": 1e3 * st["tgv_ms"] / max(st["tgv_launches"], 1), "reverse_tgv_ms": st["tgv_ms"],
-            "reverse_tgv_ms_per_level": st["tgv_ms_level"],
+            "reverse_tgv_ms_per_level": st["tgv_ms_level"], "recompute_ms": st.get("recompute_ms"),
             "traffic": (tr["dram_bytes_per_alg_byte"] * st["tgv_alg_bytes"] / max(st["tgv_launches"], 1)) if tr else None}
 
 

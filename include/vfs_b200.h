@@ -187,6 +187,7 @@ typedef struct VfsSolveStats {
   long long tgv_launches;      /* number of TGV kernel launches timed */
   int tgv_intervals;           /* event pairs summed */
   double tgv_ms_level[16];     /* tgv_ms split by pyramid level (0 = finest) */
+  double recompute_ms;         /* reverse mode: device time of the checkpoint intervals' recomputation */
 } VfsSolveStats;
 /* Statistics of the last solve; synchronise its stream first. */
 VFS_API int vfs_plan_stats(VfsPlan* plan, VfsSolveStats* out);

@@ -1149,15 +1149,17 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
     const long f = base + (long)(ry[j] + LH) * w + (rx[j] + LHX);
     const bool ok = e < N && f >= 0 && f < n;
     if (e < N) {
-      P(bCA)[e] = ok ? r.c.a[f] : 0.f;
-      P(bCB)[e] = ok ? r.c.b[f] : 0.f;
-      P(bCC)[e] = ok ? r.c.c[f] : 0.f;
-      const float ex = ok ? r.c.ex[f] : 0.f, ey = ok ? r.c.ey[f] : 0.f, ez = ok ? r.c.ez[f] : 0.f;
-      P(bREX)[e] = fabsf(ex) < eps ? 0.f : 1.f / ex;
-      P(bREY)[e] = fabsf(ey) < eps ? 0.f : 1.f / ey;
-      P(bREZ)[e] = fabsf(ez) < eps ? 0.f : 1.f / ez;
-      P(bIU)[e] = ok ? r.c.iu[f] : 0.f;
-      P(bIZ)[e] = ok ? r.c.iz[f] : 0.f;
+      // the constants as two 16-byte records per pixel (a, b, c, ex), (ey, ez, iu, iz)
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 c0 = ok ? r.c.rec[2 * f] : z, c1 = ok ? r.c.rec[2 * f + 1] : z;
+      P(bCA)[e] = c0.x;
+      P(bCB)[e] = c0.y;
+      P(bCC)[e] = c0.z;
+      P(bREX)[e] = fabsf(c0.w) < eps ? 0.f : 1.f / c0.w;
+      P(bREY)[e] = fabsf(c1.x) < eps ? 0.f : 1.f / c1.x;
+      P(bREZ)[e] = fabsf(c1.y) < eps ? 0.f : 1.f / c1.y;
+      P(bIU)[e] = c1.z;
+      P(bIZ)[e] = c1.w;
       scode[e] = ok ? r.c.code[f] : 0;
     }
   }
@@ -1523,7 +1525,7 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 // when that launch wrote none of the recorded states this one reads before
 // its griddepcontrol.wait, i.e. not right after a recomputation).
 cudaError_t launch_rev_block(int shape, const RevBlockArgs& r, cudaStream_t s, bool pdl) {
-  if (!r.k.dscale) return cudaErrorInvalidValue;  // dual-step scales not formed
+  if (!r.k.dscale || !r.c.rec) return cudaErrorInvalidValue;  // dual-step scales or constant records missing
   switch (shape) {
 #define VFS_REVB_L(ID, K, TX, TY, NT)                                              \
   case ID: {                                                                       \
@@ -2133,6 +2135,26 @@ cudaError_t zero_state(const TgvState& st, size_t n, cudaStream_t s) {
   return cudaSuccess;
 }
 
+// Timing mode: opens an event pair (its first event recorded now) for a
+// stretch of launches of level `level` (negative: a recomputation) with the
+// given algorithmic bytes and launch count.
+int timing_pair(VfsGradPlan* gp, int level, double bytes, long long launches, cudaStream_t s, int* pair) {
+  *pair = gp->tev_used++;
+  while ((int)gp->tev.size() < 2 * (*pair + 1)) {
+    cudaEvent_t e;
+    VFS_TRY_CUDA(cudaEventCreate(&e), "event create");
+    gp->tev.push_back(e);
+  }
+  gp->tev_bytes.resize(*pair + 1);
+  gp->tev_launches.resize(*pair + 1);
+  gp->tev_level.resize(*pair + 1);
+  gp->tev_bytes[*pair] = bytes;
+  gp->tev_launches[*pair] = launches;
+  gp->tev_level[*pair] = level;
+  VFS_TRY_CUDA(cudaEventRecord(gp->tev[2 * *pair], s), "event record");
+  return VFS_OK;
+}
+
 int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_other, double* g_scalars,
                   cudaStream_t s) {
   VfsPlan* pl = gp->pl;
@@ -2215,6 +2237,11 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
           nj = std::max(0, std::min(gp->ckpt, nI - it0));
           S = interval_states(gp, wt, j, nI);
           dS = wt.d_seg + (size_t)j * (gp->ckpt + 1);
+          // timing: the recomputation's own event pair, marked by a level of -1 - l
+          int rpair = -1;
+          if (gp->timing && nj > 1) {
+            VFS_TRY(timing_pair(gp, -1 - l, 0.0, 0, s, &rpair));
+          }
           if (tv) {
             for (int q = 0; q < nj - 1;) {
               const int m = std::min(tgv_max_iters_per_launch(tv), nj - 1 - q);
@@ -2230,28 +2257,18 @@ int grad_backward(VfsGradPlan* gp, const float* gdepth, float* g_ref, float* g_o
               VFS_TRY_CUDA(launch_tgv_block(1, S[q - 1], S[q], cst, pl->sched, it0 + q - 1, 1, pl->kc, h, w, s),
                            "tgv recompute");
           }
+          if (rpair >= 0) VFS_TRY_CUDA(cudaEventRecord(gp->tev[2 * rpair + 1], s), "event record");
         }
         const int form = gp->level_form[l] ? gp->level_form[l] : gp->fused_reverse;
         const int Kr = rev_block_iters(form);
         int pair = -1;
         if (gp->timing && nj > 0) {
-          pair = gp->tev_used++;
-          while ((int)gp->tev.size() < 2 * (pair + 1)) {
-            cudaEvent_t e;
-            VFS_TRY_CUDA(cudaEventCreate(&e), "event create");
-            gp->tev.push_back(e);
-          }
-          gp->tev_bytes.resize(pair + 1);
-          gp->tev_launches.resize(pair + 1);
-          gp->tev_level.resize(pair + 1);
           // algorithmic bytes of one reversed iteration, per pixel: the state
           // before (40) and the p, q after it (24), the cotangent in (40) and
           // out (40), the constants (33), the constant cotangents read and
           // written (64)
-          gp->tev_bytes[pair] = 241.0 * (double)n * nj;
-          gp->tev_launches[pair] = Kr > 0 ? (nj + Kr - 1) / Kr : (form ? nj : 3 * nj);
-          gp->tev_level[pair] = l;
-          VFS_TRY_CUDA(cudaEventRecord(gp->tev[2 * pair], s), "event record");
+          VFS_TRY(timing_pair(gp, l, 241.0 * (double)n * nj, Kr > 0 ? (nj + Kr - 1) / Kr : (form ? nj : 3 * nj), s,
+                              &pair));
         }
         if (Kr > 0) {
           for (int i1 = nj; i1 > 0;) {
@@ -2429,11 +2446,15 @@ int vfs_grad_stats(VfsGradPlan* gp, VfsSolveStats* out) {
   for (int i = 0; i < gp->tev_used; ++i) {
     float t = 0;
     VFS_TRY_CUDA(cudaEventElapsedTime(&t, gp->tev[2 * i], gp->tev[2 * i + 1]), "event elapsed (synchronise first)");
+    const int lvl = gp->tev_level[i];
+    if (lvl < 0) {  // a recomputation
+      out->recompute_ms += t;
+      continue;
+    }
     out->tgv_ms += t;
     out->tgv_alg_bytes += gp->tev_bytes[i];
     out->tgv_launches += gp->tev_launches[i];
-    const int lvl = gp->tev_level[i];
-    if (lvl >= 0 && lvl < 16) out->tgv_ms_level[lvl] += t;
+    if (lvl < 16) out->tgv_ms_level[lvl] += t;
   }
   out->tgv_intervals = gp->tev_used;
   return VFS_OK;

@@ -45,7 +45,8 @@ class VfsSolveStats(ctypes.Structure):
     """Mirror of ``VfsSolveStats`` in include/vfs_b200.h."""
     _fields_ = [("kernels_per_solve", ctypes.c_longlong), ("tgv_ms", ctypes.c_double),
                 ("tgv_alg_bytes", ctypes.c_double), ("tgv_launches", ctypes.c_longlong),
-                ("tgv_intervals", ctypes.c_int), ("tgv_ms_level", ctypes.c_double * 16)]
+                ("tgv_intervals", ctypes.c_int), ("tgv_ms_level", ctypes.c_double * 16),
+                ("recompute_ms", ctypes.c_double)]
 
 
 _P = ctypes.c_void_p

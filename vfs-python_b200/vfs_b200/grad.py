@@ -155,7 +155,7 @@ class DepthSolver:
         st = _lib.VfsSolveStats()
         call("vfs_grad_stats", self._gp, ctypes.byref(st))
         return {"tgv_ms": st.tgv_ms, "tgv_alg_bytes": st.tgv_alg_bytes, "tgv_launches": st.tgv_launches,
-                "tgv_ms_level": list(st.tgv_ms_level)[: int(self.param.nLevel)]}
+                "tgv_ms_level": list(st.tgv_ms_level)[: int(self.param.nLevel)], "recompute_ms": st.recompute_ms}
 
     def theta_of(self, param=None) -> torch.Tensor:
         p = param or self.param
