@@ -280,7 +280,10 @@ cudaError_t batch_reg(const TgvBatchParams& P, int n_tiles, int parity, const fl
 // 221 (36x36, 3 iterations, a 45x45 window, two pixels per thread) is the
 // largest square tile within 1024 x 2 window pixels: the least halo per tile
 // pixel, and 529 tiles fill four waves at 800^2 (the 32x32 tiles' 625 need
-// five).
+// five).  Ids 23x are 512-thread kernels with two pixels per thread compiled
+// for two CTAs per SM (64 registers): more halo per tile pixel than 221, but
+// each CTA's barrier waits overlap the other CTA's work; 232 (26x26, 2
+// iterations) is the fastest at 800^2.
 #define VFS_TGV_VARIANTS(X)          \
   X(1, block, 1, 32, 16, 256)        \
   X(2, block, 2, 32, 32, 512)        \
@@ -327,7 +330,14 @@ cudaError_t batch_reg(const TgvBatchParams& P, int n_tiles, int parity, const fl
   X(223, reg, 5, 17, 17, 1024)       \
   X(224, reg, 6, 9, 9, 736)          \
   X(225, reg, 4, 11, 11, 544)        \
-  X(226, reg, 4, 27, 27, 1024)
+  X(226, reg, 4, 27, 27, 1024)       \
+  X(230, reg, 3, 23, 23, 512)        \
+  X(231, reg, 4, 20, 20, 512)        \
+  X(232, reg, 2, 26, 26, 512)        \
+  X(233, reg, 3, 22, 22, 512)        \
+  X(234, reg, 2, 28, 24, 512)        \
+  X(235, reg, 2, 32, 20, 512)        \
+  X(236, reg, 2, 24, 28, 512)
 
 // Register-owned variants also compiled in recording form (every
 // iteration's state written out), for the reverse mode's recomputation.
@@ -340,7 +350,8 @@ cudaError_t batch_reg(const TgvBatchParams& P, int n_tiles, int parity, const fl
   X(220, 3, 34, 34, 1024)         \
   X(221, 3, 36, 36, 1024)         \
   X(222, 4, 17, 17, 864)          \
-  X(224, 6, 9, 9, 736)
+  X(224, 6, 9, 9, 736)            \
+  X(232, 2, 26, 26, 512)
 
 }  // namespace
 

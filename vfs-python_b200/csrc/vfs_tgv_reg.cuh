@@ -22,6 +22,15 @@ namespace {
 // the flag added to the codes of a warp whose pixels all have kAllSides
 constexpr uint8_t kWarpFull = 32;
 
+// CTAs per SM the register-owned kernels are compiled for: two for blocks of
+// up to 256 threads, and for 512-thread blocks whose threads own two window
+// pixels (64 registers each, so that two CTAs share an SM and one's barrier
+// waits overlap the other's work); one otherwise.
+template <int K, int TX, int TY, int NT>
+constexpr int reg_min_blocks() {
+  return NT <= 256 ? 2 : (NT == 512 && (TX + 3 * K) * (TY + 3 * K) > NT && (TX + 3 * K) * (TY + 3 * K) <= 2 * NT ? 2 : 1);
+}
+
 template <int K, int TX, int TY>
 struct RegGeom {
   static constexpr int WX = TX + 3 * K;
@@ -315,7 +324,7 @@ __device__ __forceinline__ void tgv_reg_tile(const TgvState& in, const TgvState&
 }
 
 template <int K, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
+__global__ void __launch_bounds__(NT, reg_min_blocks<K, TX, TY, NT>())
     k_tgv_reg(TgvState in, TgvState out, TgvConsts cst, const float3* __restrict__ sched, int it0, int niter,
               SolverConsts kc, int h, int w) {
   tgv_reg_tile<K, TX, TY, NT>(in, out, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY);
@@ -324,7 +333,7 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
 // Recording: every iteration's state to the records 0..niter of the trace
 // (record r: the planes of trace0 moved by r * rec_stride floats).
 template <int K, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
+__global__ void __launch_bounds__(NT, reg_min_blocks<K, TX, TY, NT>())
     k_tgv_reg_trace(TgvState in, TgvState trace0, long rec_stride, TgvConsts cst, const float3* __restrict__ sched,
                     int it0, int niter, SolverConsts kc, int h, int w) {
   tgv_reg_tile<K, TX, TY, NT, true>(in, trace0, cst, sched, it0, niter, kc, h, w, blockIdx.x * TX, blockIdx.y * TY,
@@ -337,7 +346,7 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
 // P.bid0 .. P.bid0 + grid - 1; block b belongs to the last item whose
 // tile_base <= b.
 template <int K, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, (NT <= 256 ? 2 : 1))
+__global__ void __launch_bounds__(NT, reg_min_blocks<K, TX, TY, NT>())
     k_tgv_reg_batch(const __grid_constant__ TgvBatchParams P, int parity, const float3* __restrict__ sched, int it0,
                     int niter, SolverConsts kc) {
   int lo = 0, hi = P.n_items - 1;
