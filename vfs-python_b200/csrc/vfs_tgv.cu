@@ -283,7 +283,9 @@ cudaError_t batch_reg(const TgvBatchParams& P, int n_tiles, int parity, const fl
 // five).  Ids 23x are 512-thread kernels with two pixels per thread compiled
 // for two CTAs per SM (64 registers): more halo per tile pixel than 221, but
 // each CTA's barrier waits overlap the other CTA's work; 232 (26x26, 2
-// iterations) is the fastest at 800^2.
+// iterations) is the fastest at 800^2.  One wave of two CTAs per SM on the
+// 400^2, 200^2 and 100^2 levels (24x24 K=2, 12x12 K=4, 8x8 K=6: 289, 289
+// and 169 tiles) measured slower there than the one-CTA shapes.
 #define VFS_TGV_VARIANTS(X)          \
   X(1, block, 1, 32, 16, 256)        \
   X(2, block, 2, 32, 32, 512)        \
