@@ -320,7 +320,8 @@ def parity_vs_reference(pair, p, flow, xyz):
 
 
 # ncu captures of the finest level's kernel, by TGV variant
-TRAFFIC_FILES = {221: "k_tgv_reg_36x36_800x800_ncu.json", 134: "k_tgv_reg_800x800_ncu.json"}
+TRAFFIC_FILES = {232: "k_tgv_reg_26x26_800x800_ncu.json", 221: "k_tgv_reg_36x36_800x800_ncu.json",
+                 134: "k_tgv_reg_800x800_ncu.json"}
 
 
 def load_traffic(name="k_tgv_reg_800x800_ncu.json"):
