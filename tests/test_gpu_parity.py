@@ -196,8 +196,9 @@ def test_solve_bit_exact_bench_params(ref_mod, n_iter):
     prm = bench_params(h, w, n_level=3, n_warp=3, n_iter=n_iter)
     from vfs_b200 import _lib
     import ctypes
-    ids = (ctypes.c_int * 64)()
-    n = _lib.lib().vfs_tgv_variants(ids, 64, None)
+    n = _lib.lib().vfs_tgv_variants(None, 0, None)
+    ids = (ctypes.c_int * n)()
+    assert _lib.lib().vfs_tgv_variants(ids, n, None) == n
     configs = [(ids[i], False) for i in range(n)] + [(134, True)]
     (rw, rxyz), outs, o, cam = _solve_pair(ref_mod, prm, p, variants=configs)
     for v, (ow, oxyz) in outs.items():

@@ -25,8 +25,9 @@ _CACHE: dict = {}
 
 
 def variants() -> list[int]:
-    ids = (ctypes.c_int * 128)()
-    n = _lib.lib().vfs_tgv_variants(ids, 128, None)
+    n = _lib.lib().vfs_tgv_variants(None, 0, None)
+    ids = (ctypes.c_int * n)()
+    n = min(n, _lib.lib().vfs_tgv_variants(ids, n, None))
     return [ids[i] for i in range(n)]
 
 
