@@ -35,6 +35,7 @@ only.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -80,6 +81,16 @@ def level_pixels(p):
 def alg_bytes_per_map(p):
     return sum(n * (p.nWarpIters * (p.nSolverIters * ALG_BYTES_ITER + ALG_BYTES_WARP) + ALG_BYTES_LEVEL)
                for n in level_pixels(p))
+
+
+def variant_iters(variant):
+    """Iterations per launch of a compiled TGV kernel variant."""
+    from vfs_b200 import _lib
+    lib = _lib.lib()
+    n = lib.vfs_tgv_variants(None, 0, None)
+    ids, its = (ctypes.c_int * n)(), (ctypes.c_int * n)()
+    lib.vfs_tgv_variants(ids, n, its)
+    return dict(zip(ids, its))[variant]
 
 
 def measured_peak():
@@ -364,7 +375,7 @@ def run_b200(args, n, rank, local):
 
     # ---- device-resident throughput
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    tgv_ms = tgv_bytes = 0.0
+    tgv_ms = tgv_ms_fine = tgv_bytes = 0.0
     tgv_launches = 0
     barrier(n)
     torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed steps (ncu --nvtx-include timed/)
@@ -376,6 +387,7 @@ def run_b200(args, n, rank, local):
             ev[i][1].record(stream)
             st = vfs.solve_stats()  # synchronises
             tgv_ms += st["tgv_ms"]
+            tgv_ms_fine += st["tgv_ms_level"][0]
             tgv_bytes += st["tgv_alg_bytes"]
             tgv_launches += st["tgv_launches"]
     torch.cuda.nvtx.range_pop()
@@ -416,12 +428,20 @@ def run_b200(args, n, rank, local):
     m = (pair.mask > 0) & (pair.depth > 0)
 
     peak, peak_kind = measured_peak()
-    achieved = tgv_bytes / (tgv_ms / 1e3) / 1e9 if tgv_ms > 0 else None
-    traffic = None
+    # the dominant kernel: the finest level's TGV kernel (one variant, one
+    # shape); its launches per solve are nWarpIters x ceil(nSolverIters / K)
+    # and each processes K iterations of every pixel of the level
     fine = level_choice[0] if level_choice else args.iters_per_launch
+    k_fine = variant_iters(fine)
+    fine_launches = N_WARP * -(-N_ITER // k_fine)
+    fine_bytes_per_launch = SIZE * SIZE * ALG_BYTES_ITER * (N_ITER * N_WARP) / fine_launches
+    fine_launch_us = 1e3 * tgv_ms_fine / (fine_launches * args.steps) if tgv_ms_fine > 0 else None
+    achieved = fine_bytes_per_launch / (fine_launch_us / 1e6) / 1e9 if fine_launch_us else None
+    all_achieved = tgv_bytes / (tgv_ms / 1e3) / 1e9 if tgv_ms > 0 else None
+    traffic = None
     tr = load_traffic(TRAFFIC_FILES[fine]) if fine in TRAFFIC_FILES else None
-    if tr and tgv_launches:
-        traffic = tr["dram_bytes_per_alg_byte"] * (tgv_bytes / tgv_launches)
+    if tr:
+        traffic = tr["dram_bytes_per_alg_byte"] * fine_bytes_per_launch
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -434,13 +454,23 @@ def run_b200(args, n, rank, local):
                    "autotune_fastest_per_level_ms_variant": tune_top,
                    "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "parallelism": f"dp{n} (independent pairs)"},
-        "roofline": {"bound": "hbm", "kernel": f"k_tgv_reg (fused TGV iterations; finest level variant {fine})",
+        "roofline": {"bound": "hbm",
+                     "kernel": f"k_tgv_reg variant {fine} (fused TGV, {k_fine} iterations per launch) on the "
+                               f"{SIZE}x{SIZE} level",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                      "traffic": traffic,
-                     "alg_bytes_per_launch": tgv_bytes / max(tgv_launches, 1),
-                     "avg_launch_us": 1e3 * tgv_ms / max(tgv_launches, 1),
-                     "tgv_share_of_step": (tgv_ms / 1e3) / elapsed if elapsed else None},
+                     "alg_bytes_per_launch": fine_bytes_per_launch, "avg_launch_us": fine_launch_us,
+                     "launches_per_step": fine_launches,
+                     "share_of_step": (tgv_ms_fine / 1e3) / elapsed if elapsed else None,
+                     "basis": "113 algorithmic bytes per pixel-iteration x the level's pixels x the launch's "
+                              "iterations, over the launches' CUDA-event time (events around each warp's TGV "
+                              "launches of the level, summed over the timed steps)",
+                     "all_tgv_levels": {"achieved": all_achieved,
+                                        "frac": (all_achieved / peak) if all_achieved else None,
+                                        "alg_bytes_per_launch": tgv_bytes / max(tgv_launches, 1),
+                                        "avg_launch_us": 1e3 * tgv_ms / max(tgv_launches, 1),
+                                        "share_of_step": (tgv_ms / 1e3) / elapsed if elapsed else None}},
         "alg_bytes_per_map": alg_bytes_per_map(p),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * SIZE * SIZE,
                 "d2h_bytes_per_step": 4 * SIZE * SIZE},

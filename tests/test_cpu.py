@@ -323,3 +323,5 @@ def test_bench_algorithmic_bytes_and_profile_files():
         d = json.load(open(os.path.join(ROOT, "profiles", name)))
         assert 0 < d["dram_bytes_per_alg_byte"] < 1
         assert abs(d["dram_bytes_per_alg_byte"] - (d["dram_read_bytes"] + d["dram_write_bytes"]) / d["alg_bytes"]) < 1e-3
+    # the dominant kernel's launches: K iterations each (no GPU needed to ask)
+    assert bench.variant_iters(232) == 2 and bench.variant_iters(221) == 3 and bench.variant_iters(134) == 4
