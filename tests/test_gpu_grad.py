@@ -214,7 +214,7 @@ def test_backward_kernel_forms_agree():
     outs = []
     forms = [(0, -1), (1, -1), (0, 0), (1, 0), (1, 124), (1, 216), (1, 220), (1, 221), (1, 222), (1, 224), (2, 0), (3, 0),
              (4, 0), (5, 0)]
-    forms += [(b, 0) for b in (11, 12, 13, 14, 15, 16, 17, 18, 19, 20)]
+    forms += [(b, 0) for b in (11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 22, 23, 24, 25)]
     for fused, tv in forms:
         s.set_options(fused, tv)
         outs.append(_gpu_grads(s, I0, I1, t, theta, wts))

@@ -1501,9 +1501,11 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
 
 // Blocked reverse configurations: id -> (iterations per launch, tile, threads).
 // One CTA per SM (registers and shared memory): 19 covers a 200^2 level
-// with 140 tiles, one wave on the 148 SMs, where 17 needs 153; 20 is the
-// widest tile whose window (36x23) fits one pixel per thread within the
-// register budget, recomputing 1.85 window pixels per tile pixel (11: 1.92).
+// with 140 tiles, one wave on the 148 SMs, where 17 needs 153; 23 (window
+// 32x28, 896 threads at 72 registers, the most that one pixel per thread
+// allows) recomputes 1.78 window pixels per tile pixel (22: 1.80, 20: 1.85,
+// 11: 1.92) and is the fastest at the 800^2 and 400^2 levels; 24 and 25 are
+// three-iteration forms of the same window size.
 // One iteration per launch with wider tiles (28x20, 32x18, 24x24 at 864-896
 // threads: 1.54 window pixels per tile pixel) measured 1.5x slower at
 // 800x800 than these forms: the constants, cotangents and states are then
@@ -1519,7 +1521,11 @@ __global__ void __launch_bounds__(NT, 1) k_rev_block(RevBlockArgs r) {
   X(17, 3, 24, 12, 800)    \
   X(18, 2, 32, 12, 768)    \
   X(19, 3, 20, 15, 800)    \
-  X(20, 2, 28, 16, 832)
+  X(20, 2, 28, 16, 832)    \
+  X(22, 2, 24, 20, 864)    \
+  X(23, 2, 24, 21, 896)    \
+  X(24, 3, 20, 18, 896)    \
+  X(25, 3, 20, 17, 864)
 
 // pdl: may start as a programmatic dependent of the previous launch (only
 // when that launch wrote none of the recorded states this one reads before

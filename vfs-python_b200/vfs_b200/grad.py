@@ -87,7 +87,7 @@ class DepthSolver:
         self.level_forms = list(forms)
 
     def autotune(self, img_ref, img_other, t, theta=None, g_depth=None,
-                 forms=(11, 20, 13, 18, 17, 19, 12, 15, 16, 14), fwd_variants=(134, 124, 212, 216, 207, 220, 221, 222, 224, 232),
+                 forms=(11, 20, 22, 23, 24, 25, 13, 18, 17, 19, 12, 15, 16, 14), fwd_variants=(134, 124, 212, 216, 207, 220, 221, 222, 224, 232),
                  repeats: int = 2):
         """Choose, per level, the recording forward's TGV kernel and then the
         reverse-step form, by timing whole passes (levels are independent, so
