@@ -715,7 +715,8 @@ def _grad_step_parts(solver, ref_f, oth_f, t, theta, gt, valid):
 
 
 # ncu captures of the reverse kernel, by reverse form
-REV_TRAFFIC_FILES = {20: "k_rev_block_28x16_800x800_ncu.json", 11: "k_rev_block_800x800_ncu.json"}
+REV_TRAFFIC_FILES = {23: "k_rev_block_24x21_800x800_ncu.json", 20: "k_rev_block_28x16_800x800_ncu.json",
+                     11: "k_rev_block_800x800_ncu.json"}
 
 
 def reverse_roofline(solver, run_once):
