@@ -289,10 +289,11 @@ VFS_API int vfs_grad_forward(VfsGradPlan* plan, const float* img_ref, const floa
 VFS_API int vfs_grad_backward(VfsGradPlan* plan, const float* g_depth, float* g_ref, float* g_other,
                               double* g_scalars, void* stream);
 /* Backward kernels: fused_reverse selects how an iteration is reversed:
- * 11..20 (default 11) two to four iterations per launch, cotangent state on chip
+ * 11..20 and 22..25 (default 11) two to four iterations per launch, cotangent state on chip
  * (11: 2 iterations, 24x16 tiles; 12: 2, 16x16; 13: 3, 16x16; 14: 4, 16x8;
  * 15: 2, 8x8; 16: 4, 8x8; 17: 3, 24x12; 18: 2, 32x12; 19: 3, 20x15;
- * 20: 2, 28x16), 1..5 one iteration per launch in one tiled kernel
+ * 20: 2, 28x16; 22: 2, 24x20; 23: 2, 24x21; 24: 3, 20x18; 25: 3, 20x17), 1..5 one
+ * iteration per launch in one tiled kernel
  * (1: 32x16; 2: 32x8; 3: 64x8; 4: 32x32; 5: 28x16), 0 three gather kernels.
  * trace_variant selects the TGV variant that recomputes checkpoint intervals
  * (0: automatic, -1: one iteration per launch).  With ckpt_every 1 the

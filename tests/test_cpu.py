@@ -325,3 +325,22 @@ def test_bench_algorithmic_bytes_and_profile_files():
         assert abs(d["dram_bytes_per_alg_byte"] - (d["dram_read_bytes"] + d["dram_write_bytes"]) / d["alg_bytes"]) < 1e-3
     # the dominant kernel's launches: K iterations each (no GPU needed to ask)
     assert bench.variant_iters(232) == 2 and bench.variant_iters(221) == 3 and bench.variant_iters(134) == 4
+
+
+def test_checkpoint_spacing_sized_to_memory():
+    """DepthSolver(ckpt_every="auto"): the densest checkpoint spacing whose
+    reverse-mode workspace fits the budget (800x800, 5 levels x 10 warps x 100
+    iterations: every state recorded needs 34.6 GB, every 10 iterations 4.1 GB;
+    the workspace is least near 50, since the backward buffers one interval)."""
+    from vfs_b200 import grad
+    from vfs_b200.vfs_params import vfs_params
+    p = vfs_params(np.zeros((800, 800), np.uint8))
+    p.nLevel, p.nWarpIters, p.nSolverIters, p.fScale = 5, 10, 100, 2.0
+    w = {k: grad.workspace_bytes(p, k) for k in grad.CKPT_CANDIDATES}
+    assert abs(w[1] - 34.589e9) < 1e7 and abs(w[10] - 4.121e9) < 1e7
+    assert grad.checkpoint_interval(p, 180e9) == 1
+    assert grad.checkpoint_interval(p, w[2]) == 2
+    assert grad.checkpoint_interval(p, w[10]) == 10
+    assert grad.checkpoint_interval(p, min(w.values())) == min(w, key=w.get)
+    with pytest.raises(MemoryError):
+        grad.checkpoint_interval(p, min(w.values()) - 1)

@@ -36,21 +36,51 @@ from ._lib import call, ptr, stream
 
 THETA = ("Lambda", "alpha0", "alpha1", "beta", "gamma")
 
+# checkpoint spacings tried by checkpoint_interval, densest first
+CKPT_CANDIDATES = (1, 2, 5, 10, 20, 25, 50, 100)
+
+
+def workspace_bytes(param, ckpt_every: int) -> int:
+    """Device workspace of a DepthSolver with this parameter bag and spacing."""
+    need = ctypes.c_size_t(0)
+    call("vfs_grad_workspace_size", ctypes.byref(_lib.VfsParams.from_param_bag(param)), int(ckpt_every),
+         ctypes.byref(need))
+    return int(need.value)
+
+
+def checkpoint_interval(param, budget_bytes: int, candidates=CKPT_CANDIDATES) -> int:
+    """The densest checkpoint spacing whose workspace fits ``budget_bytes``
+    (denser spacings recompute less in the backward: 1 records every state and
+    recomputes nothing).  The workspace is not monotonic in the spacing: sparse
+    checkpoints save the recorded states, but the backward then buffers every
+    state of one interval.  Raises MemoryError if no candidate fits."""
+    need = {int(k): workspace_bytes(param, k) for k in candidates}
+    for k in sorted(need):
+        if need[k] <= budget_bytes:
+            return k
+    k_min = min(need, key=need.get)
+    raise MemoryError(f"no checkpoint spacing in {tuple(sorted(need))} fits {int(budget_bytes)} bytes "
+                      f"(the least, every {k_min} iterations, needs {need[k_min]})")
+
 
 class DepthSolver:
-    def __init__(self, param, camera, mask, t_scale: float = 1.0, ckpt_every: int = 10, level_variants=None,
-                 triangulation: str = "reference"):
+    def __init__(self, param, camera, mask, t_scale: float = 1.0, ckpt_every=10, level_variants=None,
+                 triangulation: str = "reference", memory_budget: int | None = None):
         """``triangulation``: "reference" (the reference's x-only formula) or
         "lsq" (least squares along the reference ray, all of t; the choice for
-        baselines with large y or z components)."""
+        baselines with large y or z components).  ``ckpt_every="auto"`` sizes
+        the checkpointing to the memory: the densest spacing whose workspace
+        fits ``memory_budget`` bytes (default: 90 % of the device memory free
+        now; give each of several solvers its share)."""
         if triangulation not in ("reference", "lsq"):
             raise ValueError(f"triangulation {triangulation!r}: use 'reference' or 'lsq'")
         self.param = param
         self.prm = _lib.VfsParams.from_param_bag(param)
+        if ckpt_every == "auto":
+            budget = memory_budget if memory_budget is not None else int(0.9 * torch.cuda.mem_get_info()[0])
+            ckpt_every = checkpoint_interval(param, budget)
         self.ckpt_every = int(ckpt_every)
-        need = ctypes.c_size_t(0)
-        call("vfs_grad_workspace_size", ctypes.byref(self.prm), self.ckpt_every, ctypes.byref(need))
-        self.workspace_bytes = int(need.value)
+        self.workspace_bytes = workspace_bytes(param, self.ckpt_every)
         self._ws = torch.empty(self.workspace_bytes + 1024, dtype=torch.uint8, device="cuda")
         gp = ctypes.c_void_p(0)
         f, u0, v0 = camera._k() if hasattr(camera, "_k") else (float(x) for x in camera)
@@ -75,7 +105,7 @@ class DepthSolver:
 
     def set_options(self, fused_reverse: int = 11, trace_variant: int = 0) -> None:
         """Backward kernel forms (see vfs_grad_set_options in vfs_b200.h): the
-        reverse-step kernel (11..20 two to four iterations per launch, 1..5 one
+        reverse-step kernel (11..20, 22..25 two to four iterations per launch, 1..5 one
         tiled kernel per iteration, 0 three gather kernels) and the TGV variant
         recomputing checkpoint intervals (0 automatic, -1 one iteration per launch)."""
         call("vfs_grad_set_options", self._gp, int(fused_reverse), int(trace_variant))
