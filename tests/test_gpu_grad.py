@@ -229,6 +229,25 @@ def test_backward_kernel_forms_agree():
             assert _rel(a, b) < 1e-5
 
 
+def test_checkpointing_sized_to_memory():
+    """ckpt_every="auto" picks the densest spacing whose workspace fits the
+    budget and gives the gradients of that spacing chosen by hand."""
+    from vfs_b200 import DepthSolver, EquidistantCam, grad
+    P, prm, I0, I1 = _problem(n_iter=9)
+    t = P.t.reshape(3).astype(np.float64)
+    theta = _theta(prm)
+    budget = grad.workspace_bytes(prm, 5)
+    auto = DepthSolver(prm, EquidistantCam(P.intrinsics), P.mask, ckpt_every="auto", memory_budget=budget)
+    assert auto.ckpt_every == grad.checkpoint_interval(prm, budget) and auto.workspace_bytes <= budget
+    d = _gpu_grads(auto, I0, I1, t, theta, np.zeros(I0.shape))[0]
+    good = (P.mask != 0) & np.isfinite(d) & (np.abs(d) < 30)
+    wts = np.where(good, np.random.default_rng(3).normal(0, 1, good.shape), 0.0) * 1e-3
+    got = _gpu_grads(auto, I0, I1, t, theta, wts)
+    want = _gpu_grads(_solver(P, prm, ckpt=auto.ckpt_every), I0, I1, t, theta, wts)
+    for a, b in zip(got[1:], want[1:]):
+        assert _rel(a, b) < 1e-5
+
+
 @pytest.mark.parametrize("size,seed,n_iter,noisy", [(512, 6, 30, False), (256, 0, 50, True)])
 def test_grad_finite_next_to_nan_flow(size, seed, n_iter, noisy):
     """On these pairs the forward flow is NaN at a few pixels (41 at 512x512,
