@@ -84,13 +84,14 @@ def alg_bytes_per_map(p):
 
 
 def variant_iters(variant):
-    """Iterations per launch of a compiled TGV kernel variant."""
+    """Iterations per launch of a compiled TGV kernel variant (0 for an id
+    that is not one, such as the cluster-resident kernel's)."""
     from vfs_b200 import _lib
     lib = _lib.lib()
     n = lib.vfs_tgv_variants(None, 0, None)
     ids, its = (ctypes.c_int * n)(), (ctypes.c_int * n)()
     lib.vfs_tgv_variants(ids, n, its)
-    return dict(zip(ids, its))[variant]
+    return dict(zip(ids, its)).get(variant, 0)
 
 
 def measured_peak():
@@ -432,7 +433,7 @@ def run_b200(args, n, rank, local):
     # shape); its launches per solve are nWarpIters x ceil(nSolverIters / K)
     # and each processes K iterations of every pixel of the level
     fine = level_choice[0] if level_choice else args.iters_per_launch
-    k_fine = variant_iters(fine)
+    k_fine = variant_iters(fine) or N_ITER  # the cluster-resident kernel: one launch per warp
     fine_launches = N_WARP * -(-N_ITER // k_fine)
     fine_bytes_per_launch = SIZE * SIZE * ALG_BYTES_ITER * (N_ITER * N_WARP) / fine_launches
     fine_launch_us = 1e3 * tgv_ms_fine / (fine_launches * args.steps) if tgv_ms_fine > 0 else None

@@ -344,3 +344,9 @@ def test_checkpoint_spacing_sized_to_memory():
     assert grad.checkpoint_interval(p, min(w.values())) == min(w, key=w.get)
     with pytest.raises(MemoryError):
         grad.checkpoint_interval(p, min(w.values()) - 1)
+
+
+def test_bench_variant_iters_of_non_variant():
+    """The cluster-resident kernel's id is not a tile variant: 0 iterations."""
+    import bench
+    assert bench.variant_iters(1000) == 0
